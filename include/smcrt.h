@@ -1,0 +1,282 @@
+/*
+ * smcrt.h -- C ABI of the B200 photon-packet transport library (libsmcrt_b200.so).
+ *
+ * This is the drop-in boundary for signedMCRT's per-packet transport loop.
+ * signedMCRT (Fortran 2018) runs that loop inside
+ *     subroutine pathlength_scatter(input_file)   src/kernelsMod.f90:165-333
+ *     subroutine weight_scatter(input_file)       src/kernelsMod.f90:12-163
+ *     subroutine test_kernel(input_file, end_early) src/kernelsMod.f90:335-448
+ * between `setup(...)` (:236) and `finalise(...)` (:332).  The Fortran types on
+ * that path (polymorphic class(sdf_base) allocatables, procedure pointers,
+ * module-global state/jmean) are not C-interoperable, so the caller flattens them
+ * into the plain structs below once per simulation and calls smcrt_create /
+ * smcrt_run.  Every pointer is a plain host pointer unless the name says _dev.
+ * No function exits or aborts the process: failures return a nonzero status and
+ * smcrt_last_error() returns the message (thread-local).
+ *
+ * Conventions
+ *  - Regions are the entries of the reference's `type(sdf) :: array(:)` in array
+ *    order; array order sets priority at boundary crossings
+ *    (src/inttau2.f90:131-136) and at launch (src/kernelsMod.f90:275-280).
+ *    Region-valued fields here (detector.layer, packet layer) are 1-based, as in
+ *    the reference (`packet%layer` is the array index).
+ *  - Affine transforms use the reference's row-vector convention
+ *    (src/vector_class.f90:292-304): p'_j = sum_i p_i*M[i][j] + M[3][j], i.e. the
+ *    first three columns of the reference's 4x4 `transform`, stored row-major as
+ *    M[4][3].  Build them exactly as the reference does (e.g. invert(translate(c))).
+ *  - Fluence grids are nxg*nyg*nzg doubles in Fortran column-major order,
+ *    idx = (i-1) + nxg*((j-1) + nyg*(k-1)), matching `jmean(nxg,nyg,nzg)`
+ *    (src/iarray.f90:12).  Values are the raw path-length tally (not normalised;
+ *    see normalise_fluence, src/writer.f90:25-50).
+ */
+#ifndef SMCRT_H
+#define SMCRT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMCRT_ABI_VERSION 1
+
+/* ---- status codes -------------------------------------------------------- */
+enum smcrt_status {
+    SMCRT_OK = 0,
+    SMCRT_ERR_ARG = 1,        /* bad argument (null pointer, size out of range) */
+    SMCRT_ERR_SCENE = 2,      /* invalid scene (unknown kind, bad ranges, too large) */
+    SMCRT_ERR_CUDA = 3,       /* a CUDA runtime call failed */
+    SMCRT_ERR_DEVICE = 4,     /* the kernel raised a device status flag (see stats) */
+    SMCRT_ERR_TIMEOUT = 5,    /* the host wait on the kernel ran out of time */
+    SMCRT_ERR_NO_DEVICE = 6   /* no CUDA device visible */
+};
+
+/* ---- SDF primitives (src/sdfs/sdfs.f90:494-735) --------------------------- */
+enum smcrt_prim_kind {
+    SMCRT_SPHERE = 1,   /* params: [radius]                                 sdfs.f90:494-508 */
+    SMCRT_BOX = 2,      /* params: [hx,hy,hz] half lengths (box_init halves) sdfs.f90:510-525 */
+    SMCRT_TORUS = 3,    /* params: [oradius, iradius]                        sdfs.f90:527-542 */
+    SMCRT_CYLINDER = 4, /* params: [ax,ay,az, bx,by,bz, radius]              sdfs.f90:544-581 */
+    SMCRT_TRIPRISM = 5, /* params: [h1, h2]                                  sdfs.f90:583-597 */
+    SMCRT_SEGMENT = 6,  /* params: [ax,ay,az, bx,by,bz] (radius fixed 0.1)   sdfs.f90:599-626 */
+    SMCRT_CAPSULE = 7,  /* params: [ax,ay,az, bx,by,bz, r]                   sdfs.f90:628-648 */
+    SMCRT_CONE = 8,     /* params: [ax,ay,az, bx,by,bz, ra, rb]              sdfs.f90:650-686 */
+    SMCRT_EGG = 9,      /* params: [r1, r2, h]                               sdfs.f90:688-718 */
+    SMCRT_PLANE = 10    /* params: [ax,ay,az] (normalised normal)            sdfs.f90:720-735 */
+};
+
+/* CSG fold of a model's children (src/sdfs/sdfModifiers.f90:412-475, eval_model
+ * src/sdfs/sdf_base.f90:145-160): d = child0; d = op(d, child_i, k). */
+enum smcrt_csg_op {
+    SMCRT_OP_NONE = 0,
+    SMCRT_OP_UNION = 1,
+    SMCRT_OP_SMOOTH_UNION = 2,
+    SMCRT_OP_SUBTRACTION = 3,
+    SMCRT_OP_INTERSECTION = 4
+};
+
+typedef struct smcrt_prim {
+    int32_t kind;          /* smcrt_prim_kind */
+    int32_t reserved;
+    double transform[4][3];
+    double params[8];
+} smcrt_prim;
+
+/* One entry of the reference's sdf array: a single primitive (nprims == 1) or a
+ * model (nprims > 1, folded with `op`), with its mono optical properties
+ * (init_mono, src/opticalProps/opticalProperties.f90:107-125). */
+typedef struct smcrt_region {
+    int32_t first_prim;
+    int32_t nprims;
+    int32_t op;            /* smcrt_csg_op; ignored when nprims == 1 */
+    int32_t layer_id;      /* the reference's sdf%layer (informational) */
+    double k;              /* op parameter (smooth-union width) */
+    double mus, mua, hgg, n;
+} smcrt_region;
+
+typedef struct smcrt_scene {
+    int32_t nregions;
+    int32_t nprims;
+    const smcrt_region* regions;
+    const smcrt_prim* prims;
+} smcrt_scene;
+
+/* cart_grid (src/grid.f90:14-25, init_grid :53-93): voxel counts and HALF sizes. */
+typedef struct smcrt_grid {
+    int32_t nxg, nyg, nzg, reserved;
+    double xmax, ymax, zmax;
+} smcrt_grid;
+
+/* ---- sources (src/photon.f90) --------------------------------------------- */
+enum smcrt_source_kind {
+    SMCRT_SRC_POINT = 1,    /* photon.f90:290-338, 2 draws */
+    SMCRT_SRC_PENCIL = 2,   /* photon.f90:464-505, 0 draws */
+    SMCRT_SRC_UNIFORM = 3,  /* photon.f90:397-461, 2 draws */
+    SMCRT_SRC_CIRCULAR = 4, /* photon.f90:214-287, 2 draws */
+    SMCRT_SRC_ANNULUS = 5,  /* photon.f90:645-711, 2 draws (tophat) / 2 per trial (gaussian) */
+    SMCRT_SRC_FOCUS = 6     /* photon.f90:340-394, 2 draws */
+};
+enum smcrt_annulus_type { SMCRT_ANNULUS_TOPHAT = 0, SMCRT_ANNULUS_GAUSSIAN = 1 };
+
+typedef struct smcrt_source {
+    int32_t kind;          /* smcrt_source_kind */
+    int32_t annulus_type;  /* smcrt_annulus_type */
+    double pos[3];         /* [source] position (photon_origin%pos) */
+    double dir[3];         /* [source] direction (photon_origin%nxp..nzp) */
+    double point1[3], point2[3], point3[3]; /* uniform source corners */
+    double radius;         /* circular radius / annulus inner radius ("radius") */
+    double radius_hi;      /* annulus outer radius ("radius_hi") */
+    double beta;           /* annulus beam angle in degrees ("beta") */
+    double z_inset;        /* annulus/focus start = grid zmax - z_inset; reference hard-codes 1e-8 */
+} smcrt_source;
+
+/* ---- detectors (src/detectors/detectors.f90) ------------------------------ */
+enum smcrt_detector_kind {
+    SMCRT_DET_CIRCLE = 1,   /* detectors.f90:74-127, nbins+1 bins, width maxval/(nbins-1) */
+    SMCRT_DET_ANNULUS = 2,  /* detectors.f90:129-184, nbins+1 bins, width maxval/nbins */
+    SMCRT_DET_CAMERA = 3    /* detectors.f90:186-253, (nbins+1)^2 bins, column-major */
+};
+
+typedef struct smcrt_detector {
+    int32_t kind;          /* smcrt_detector_kind */
+    int32_t layer;         /* 1-based region index the packet must end in */
+    int32_t nbins;         /* as given in the TOML (the detector holds nbins+1 bins) */
+    int32_t reserved;
+    double pos[3];         /* centre (circle/annulus) or corner p1 (camera) */
+    double dir[3];         /* normal (circle is normalised by the caller, as parse does) */
+    double r1, r2;         /* circle: r1 = radius; annulus: r1..r2 */
+    double maxval;
+    double p2[3], p3[3];   /* camera corners */
+} smcrt_detector;
+
+/* ---- run options ---------------------------------------------------------- */
+enum smcrt_kernel_kind {
+    SMCRT_KERNEL_PATHLENGTH = 0, /* pathlength_scatter: analog absorption, path-length tally */
+    SMCRT_KERNEL_WEIGHT = 1,     /* weight_scatter: implicit capture + roulette */
+    SMCRT_KERNEL_TEST = 2        /* test_kernel: scatter-order position moments */
+};
+enum smcrt_precision { SMCRT_FP32 = 0, SMCRT_FP64 = 1 };
+
+typedef struct smcrt_options {
+    int32_t kernel;        /* smcrt_kernel_kind */
+    int32_t precision;     /* transport arithmetic; tallies are always FP64 */
+    int32_t end_early;     /* test kernel: kill after the 4th scatter (test_scat.f90:65) */
+    int32_t block_size;    /* 0 = library default */
+    int32_t blocks_per_sm; /* 0 = library default (persistent grid = SMs * this) */
+    int32_t max_trace_steps; /* per tauint2 sphere-trace step cap; 0 = 1,000,000 */
+    double eps;            /* surface epsilon; <= 0 selects the default policy:
+                              1e-8 (FP64, the reference value, inttau2.f90:44) or
+                              max(1e-8, 8 ulp(largest grid half-size)) in FP32 */
+    double normal_h;       /* finite-difference step of the normal; <= 0 -> 1e-6
+                              (sdf_base.f90:176); normals are evaluated in FP64 */
+    uint32_t instance;     /* RNG stream id (second counter word) */
+    int32_t timeout_ms;    /* host wait limit for smcrt_run; 0 = 600000 */
+    void* stream;          /* cudaStream_t to launch on; NULL = a stream owned by ctx */
+} smcrt_options;
+
+/* Event counters of one run (definitions identical in the CPU oracle). */
+typedef struct smcrt_stats {
+    double nscatt;               /* sum of scatters (kernelsMod.f90:292) */
+    uint64_t packets;            /* packets launched */
+    uint64_t sdf_evals;          /* primitive-region evaluations, packet%cnts semantics
+                                    (inttau2.f90:55,90,108,121) + 4 per normal */
+    uint64_t voxel_segments;     /* tally additions in update_grids */
+    uint64_t trace_steps;        /* sphere-tracing steps */
+    uint64_t scatters;           /* scatter calls */
+    uint64_t fresnel_events;     /* reflect_refract calls */
+    uint64_t reflections;        /* of which reflected */
+    uint64_t kills_step_cap;     /* packets killed by the trace-step cap */
+    uint64_t kills_error;        /* "should not be reached" states (inttau2.f90:156) */
+    uint64_t rng_draws;          /* uniform draws consumed */
+    double moments[24];          /* test kernel: sum pos (4x3) then sum pos^2 (4x3) */
+    double kernel_ms;            /* device time of the transport kernel(s) */
+    int32_t device_status;       /* 0 or a bitmask of device status flags */
+    int32_t reserved;
+} smcrt_stats;
+
+/* Per-packet final state (history replay). */
+typedef struct smcrt_packet_state {
+    double pos[3];
+    double dir[3];
+    double weight;
+    int32_t layer;         /* 1-based */
+    int32_t nscatt;
+    int32_t ndraws;        /* uniforms consumed */
+    int32_t flags;         /* bit0 step cap, bit1 error state, bit2 stream exhausted */
+} smcrt_packet_state;
+
+typedef struct smcrt_ctx smcrt_ctx;
+
+/* Library identity. */
+int32_t smcrt_abi_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char* smcrt_last_error(void);
+
+/* Validates and uploads the flattened scene; replaces setup()'s geometry hand-off
+ * (src/kernelsMod.f90:453-546 -> setup_simulation, src/setup.f90:14-54). */
+int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid,
+                     const smcrt_source* source, const smcrt_detector* dets,
+                     int32_t ndet, const smcrt_options* opts, smcrt_ctx** out);
+void smcrt_destroy(smcrt_ctx* ctx);
+
+/* Number of detector bins of the context (sum over detectors). */
+int64_t smcrt_detector_bins(const smcrt_ctx* ctx);
+
+/* Runs packets [0, nphotons) of stream `seed` -- the OpenMP packet loop
+ * src/kernelsMod.f90:265-321 -- and copies the tallies to HOST buffers.
+ * jmean (nxg*nyg*nzg) and det_bins (smcrt_detector_bins) are overwritten; either
+ * may be NULL to skip it.  Blocks until done. */
+int32_t smcrt_run(smcrt_ctx* ctx, int64_t nphotons, uint64_t seed,
+                  double* jmean, double* det_bins, smcrt_stats* stats);
+
+/* Device-resident form: ADDS the tallies of packets [first, first+count) into
+ * caller-owned DEVICE buffers, asynchronously on the context stream.  Used for
+ * sharding packet ranges and for timing with data already in HBM.  stats may be
+ * NULL; if not NULL the call synchronises to fill it. */
+int32_t smcrt_run_device(smcrt_ctx* ctx, int64_t first, int64_t count, uint64_t seed,
+                         double* jmean_dev, double* det_bins_dev, smcrt_stats* stats);
+
+/* Replays packets from caller-supplied uniform streams instead of the counter
+ * RNG: packet p consumes uniforms[offsets[p] .. offsets[p+1]) in the reference's
+ * draw order -- emitter draws, tau (inttau2.f90:46), then per Fresnel crossing
+ * the reflect test (surfaces.f90:33) and a new tau (inttau2.f90:168), per
+ * interaction the albedo test (kernelsMod.f90:287), the bias test if g != 0
+ * (photon.f90:739), the HG/isotropic draw, the phi draw, and the next tau.
+ * Writes per-packet final states. */
+int32_t smcrt_replay(smcrt_ctx* ctx, const double* uniforms, const int64_t* offsets,
+                     int64_t npackets, double* jmean, double* det_bins,
+                     smcrt_packet_state* states, smcrt_stats* stats);
+
+/* Batched: ninst independent contexts (same precision/kernel) run in ONE
+ * persistent launch with uneven packet counts.  jmeans[i]/bins[i] are host
+ * buffers (or NULL). */
+int32_t smcrt_run_batched(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* nphotons,
+                          const uint64_t* seeds, double* const* jmeans,
+                          double* const* det_bins, smcrt_stats* stats);
+
+/* ---- device-function probes (parity of the building blocks) --------------- */
+/* Evaluates every region's SDF at npts points (xyz triples); out[p*nregions+r]. */
+int32_t smcrt_eval_sdf(const smcrt_scene* scene, int32_t precision,
+                       const double* pts, int64_t npts, double* out);
+/* calcNormal (src/sdfs/sdf_base.f90:165-189) of one region at npts points. */
+int32_t smcrt_calc_normal(const smcrt_scene* scene, int32_t region0, double h,
+                          const double* pts, int64_t npts, double* out_xyz);
+/* fresnel (src/surfaces.f90:86-120) per (I, N, n1, n2) tuple. */
+int32_t smcrt_fresnel(int32_t precision, const double* I, const double* N,
+                      const double* n1, const double* n2, int64_t n, double* R);
+/* reflect_refract (src/surfaces.f90:14-40) with a given uniform u per tuple:
+ * writes the new direction and reflect flag. */
+int32_t smcrt_reflect_refract(int32_t precision, const double* I, const double* N,
+                              const double* n1, const double* n2, const double* u,
+                              int64_t n, double* I_out, int32_t* reflected);
+/* scatter (src/photon.f90:713-779) with given uniforms (3 per call if g != 0,
+ * else 2 (the bias-test draw is skipped when g == 0)). */
+int32_t smcrt_scatter_dir(int32_t precision, const double* dir_in, const double* g,
+                          const double* u, int64_t n, double* dir_out);
+/* Philox4x32-10 block for (key, counter): 4 words per request. */
+int32_t smcrt_philox(const uint32_t* key2, const uint32_t* ctr4, int64_t n, uint32_t* out4);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SMCRT_H */

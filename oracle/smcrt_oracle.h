@@ -1,0 +1,67 @@
+/*
+ * smcrt_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * C ABI of the CPU oracle: a C++17 restatement of signedMCRT's photon-packet
+ * transport path, used by tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline as the checker.  Nothing in the product links or calls it.
+ * Scene, grid, source and detector inputs reuse the product's flattened structs
+ * from include/smcrt.h so both sides are fed identical data.
+ */
+#ifndef SMCRT_ORACLE_H
+#define SMCRT_ORACLE_H
+
+#include <stdint.h>
+#include "../include/smcrt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_policy {
+    int32_t precision;      /* SMCRT_FP32 / SMCRT_FP64 arithmetic of the transport */
+    int32_t ref_dda;        /* 1: update_pos/update_voxels snapping DDA (inttau2.f90:213-441)
+                               0: integer-stepping DDA (the GPU's) */
+    int32_t crossing_f64;   /* 1: normal + Fresnel + reflect/refract in FP64 (the GPU's FP32 path) */
+    int32_t tally_f32;      /* 1: accumulate jmean in FP32 like the reference (iarray.f90:12) */
+    int32_t threads;        /* OpenMP threads; 0 = all */
+    int32_t reserved;
+    double eps;             /* surface epsilon (reference 1e-8) */
+    double delta;           /* voxel snap (reference 1e-8, inttau2.f90:239) */
+    double normal_h;        /* calcNormal step (reference 1e-6) */
+    int64_t max_trace_steps;/* sphere-trace step cap per tauint2 (0 = 1,000,000) */
+} oracle_policy;
+
+int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* src,
+                   const smcrt_detector* dets, int32_t ndet, int32_t kernel, int32_t end_early,
+                   const oracle_policy* pol, int64_t first, int64_t count, uint64_t seed,
+                   uint32_t instance, const double* uniforms, const int64_t* offsets,
+                   double* jmean, double* det_bins, smcrt_stats* stats,
+                   smcrt_packet_state* states);
+
+int64_t oracle_detector_bins(const smcrt_detector* dets, int32_t ndet);
+
+int32_t oracle_eval_sdf(const smcrt_scene* scene, int32_t precision, const double* pts,
+                        int64_t npts, double* out);
+int32_t oracle_calc_normal(const smcrt_scene* scene, int32_t region0, double h,
+                           const double* pts, int64_t npts, double* out_xyz);
+int32_t oracle_fresnel(int32_t precision, const double* I, const double* N, const double* n1,
+                       const double* n2, int64_t n, double* R);
+int32_t oracle_reflect_refract(int32_t precision, const double* I, const double* N,
+                               const double* n1, const double* n2, const double* u, int64_t n,
+                               double* I_out, int32_t* reflected);
+int32_t oracle_scatter_dir(int32_t precision, const double* dir_in, const double* g,
+                           const double* u, int64_t n, double* dir_out);
+int32_t oracle_philox(const uint32_t* key2, const uint32_t* ctr4, int64_t n, uint32_t* out4);
+/* Emits npk packets (ids first..) and reports launch position/direction/layer (1-based). */
+int32_t oracle_emit(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* src,
+                    int32_t precision, int64_t first, int64_t npk, uint64_t seed,
+                    double* pos, double* dir, int32_t* layer);
+/* Detector hit test + bin of one hit (record_hit_1D/2D); returns global bin or -1. */
+int64_t oracle_detector_bin(const smcrt_detector* dets, int32_t ndet, int32_t det,
+                            const double* pos, const double* dir, double value, int32_t layer1);
+int32_t oracle_max_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,664 @@
+// smcrt_api.cu -- the C ABI of include/smcrt.h.
+//
+// The context owns device memory and a stream; a run zeroes the device tallies,
+// launches the persistent transport kernel (one CTA set sized to the SM count x
+// resident CTAs per SM), waits with a host-side time limit, and copies the FP64
+// tallies out.  No call exits the process: errors return a status and a message.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "smcrt_launch.h"
+
+using namespace smcrt;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                         \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return fail(SMCRT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));             \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+int validate_scene(const smcrt_scene* s) {
+    if (!s || !s->regions || !s->prims) return fail(SMCRT_ERR_ARG, "scene: null pointer");
+    if (s->nregions <= 0 || s->nprims <= 0) return fail(SMCRT_ERR_SCENE, "scene: empty");
+    if (s->nregions > kMaxRegions || s->nprims > kMaxPrims)
+        return fail(SMCRT_ERR_SCENE, "scene: at most " + std::to_string(kMaxRegions) + " regions and " +
+                                         std::to_string(kMaxPrims) + " primitives");
+    for (int i = 0; i < s->nprims; ++i)
+        if (s->prims[i].kind < SMCRT_SPHERE || s->prims[i].kind > SMCRT_PLANE)
+            return fail(SMCRT_ERR_SCENE, "scene: unknown primitive kind at " + std::to_string(i));
+    for (int i = 0; i < s->nregions; ++i) {
+        const smcrt_region& r = s->regions[i];
+        if (r.nprims <= 0 || r.first_prim < 0 || r.first_prim + r.nprims > s->nprims)
+            return fail(SMCRT_ERR_SCENE, "scene: region " + std::to_string(i) + " primitive range out of bounds");
+        if (r.nprims > 1 && (r.op < SMCRT_OP_UNION || r.op > SMCRT_OP_INTERSECTION))
+            return fail(SMCRT_ERR_SCENE, "scene: region " + std::to_string(i) + " has an unknown CSG op");
+        if (r.nprims > 1 && r.op == SMCRT_OP_SMOOTH_UNION && !(r.k > 0))
+            return fail(SMCRT_ERR_SCENE, "scene: smooth union needs k > 0");
+    }
+    return SMCRT_OK;
+}
+
+// Optical properties only matter to transport (the probes accept the
+// reference's mono(0,0,0,0) test objects).
+int validate_optics(const smcrt_scene* s) {
+    for (int i = 0; i < s->nregions; ++i) {
+        const smcrt_region& r = s->regions[i];
+        if (!(r.mus >= 0) || !(r.mua >= 0) || !(r.n > 0) || !(r.mus + r.mua >= 0) || !std::isfinite(r.hgg) ||
+            !(std::fabs(r.hgg) < 1.0))
+            return fail(SMCRT_ERR_SCENE, "scene: region " + std::to_string(i) +
+                                             " needs mus >= 0, mua >= 0, n > 0 and |g| < 1");
+    }
+    return SMCRT_OK;
+}
+
+template <class R>
+void fill_grid(GridT<R>& g, const smcrt_grid& s) {
+    g.nx = s.nxg;
+    g.ny = s.nyg;
+    g.nz = s.nzg;
+    g.xmax = (R)s.xmax;
+    g.ymax = (R)s.ymax;
+    g.zmax = (R)s.zmax;
+    g.vx = (R)2 * (R)s.xmax / (R)s.nxg;
+    g.vy = (R)2 * (R)s.ymax / (R)s.nyg;
+    g.vz = (R)2 * (R)s.zmax / (R)s.nzg;
+    g.sx = (R)s.nxg / ((R)2 * (R)s.xmax);
+    g.sy = (R)s.nyg / ((R)2 * (R)s.ymax);
+    g.sz = (R)s.nzg / ((R)2 * (R)s.zmax);
+    g.xmax_d = s.xmax;
+    g.ymax_d = s.ymax;
+    g.zmax_d = s.zmax;
+}
+
+template <class R>
+void fill_source(SourceT<R>& d, const smcrt_source& s, const smcrt_grid& g) {
+    std::memset(&d, 0, sizeof(d));
+    d.kind = s.kind;
+    d.annulus_type = s.annulus_type;
+    for (int a = 0; a < 3; ++a) {
+        d.pos[a] = (R)s.pos[a];
+        d.dir[a] = (R)s.dir[a];
+        d.p1[a] = (R)s.point1[a];
+        d.p2[a] = (R)s.point2[a];
+        d.p3[a] = (R)s.point3[a];
+    }
+    d.radius = (R)s.radius;
+    d.radius_hi = (R)s.radius_hi;
+    const double ang = s.beta * kPI / 180.0;
+    d.sin_beta = (R)std::sin(ang);
+    d.cos_beta = (R)std::cos(ang);
+    d.zstart = (R)(g.zmax - s.z_inset);
+    // circular source: rotationAlign(a, b) (src/sdfs/sdfHelpers.f90:114-140), a = x or z axis
+    double bl = std::sqrt(s.dir[0] * s.dir[0] + s.dir[1] * s.dir[1] + s.dir[2] * s.dir[2]);
+    double b[3] = {s.dir[0] / bl, s.dir[1] / bl, s.dir[2] / bl};
+    double a[3] = {1, 0, 0};
+    d.circ_swap = 0;
+    if (std::fabs(b[0]) == 1.0 && b[1] == 0.0 && b[2] == 0.0) {
+        a[0] = 0;
+        a[2] = 1;
+        d.circ_swap = 1;
+    }
+    double v[3] = {a[1] * b[2] - a[2] * b[1], -a[0] * b[2] + a[2] * b[0], a[0] * b[1] - a[1] * b[0]};
+    double c = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    double k = 1.0 / (1.0 + c);
+    double V[3][3] = {{0, v[2], -v[1]}, {-v[2], 0, v[0]}, {v[1], -v[0], 0}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s2 = 0;
+            for (int q = 0; q < 3; ++q) s2 += V[i][q] * V[q][j];
+            d.rot[3 * i + j] = (R)((i == j ? 1.0 : 0.0) + V[i][j] + s2 * k);
+        }
+}
+
+int fill_dets(DetT* out, const smcrt_detector* dets, int ndet, int nregions, long long& total) {
+    total = 0;
+    for (int i = 0; i < ndet; ++i) {
+        DetT& D = out[i];
+        std::memset(&D, 0, sizeof(D));
+        const smcrt_detector& s = dets[i];
+        if (s.kind < SMCRT_DET_CIRCLE || s.kind > SMCRT_DET_CAMERA)
+            return fail(SMCRT_ERR_ARG, "detector " + std::to_string(i) + ": unknown kind");
+        if (s.nbins < 0) return fail(SMCRT_ERR_ARG, "detector " + std::to_string(i) + ": nbins < 0");
+        if (s.layer < 1 || s.layer > nregions)
+            return fail(SMCRT_ERR_ARG, "detector " + std::to_string(i) + ": layer outside 1..nregions");
+        D.kind = s.kind;
+        D.layer = s.layer;
+        D.off = total;
+        for (int a = 0; a < 3; ++a) {
+            D.pos[a] = s.pos[a];
+            D.dir[a] = s.dir[a];
+        }
+        D.r1 = s.r1;
+        D.r2 = s.r2;
+        D.nb = s.nbins + 1;
+        if (s.kind == SMCRT_DET_CAMERA) {  // init_camera, detectors.f90:186-229
+            D.bw = D.bwy = (s.nbins == 0) ? 1.0 : s.maxval / (double)D.nb;
+            for (int a = 0; a < 3; ++a) {
+                D.e1[a] = s.p2[a] - s.pos[a];
+                D.e2[a] = s.p3[a] - s.pos[a];
+            }
+            D.width = std::sqrt(D.e1[0] * D.e1[0] + D.e1[1] * D.e1[1] + D.e1[2] * D.e1[2]);
+            D.height = std::sqrt(D.e2[0] * D.e2[0] + D.e2[1] * D.e2[1] + D.e2[2] * D.e2[2]);
+            double nx = D.e2[1] * D.e1[2] - D.e2[2] * D.e1[1];
+            double ny = -D.e2[0] * D.e1[2] + D.e2[2] * D.e1[0];
+            double nz = D.e2[0] * D.e1[1] - D.e2[1] * D.e1[0];
+            double ln = std::sqrt(nx * nx + ny * ny + nz * nz);
+            D.n[0] = nx / ln;
+            D.n[1] = ny / ln;
+            D.n[2] = nz / ln;
+            total += (long long)D.nb * D.nb;
+        } else {
+            if (s.nbins == 0) D.bw = 1.0;
+            else if (s.kind == SMCRT_DET_CIRCLE) D.bw = s.maxval / (double)(s.nbins - 1);  // :104
+            else D.bw = s.maxval / (double)s.nbins;                                          // :163
+            total += D.nb;
+        }
+    }
+    return SMCRT_OK;
+}
+
+double default_eps(int precision, const smcrt_grid& g) {
+    if (precision == SMCRT_FP64) return 1e-8;
+    double L = std::fmax(g.xmax, std::fmax(g.ymax, g.zmax));
+    int e;
+    std::frexp(L, &e);                  // L in [2^(e-1), 2^e)
+    double ulp = std::ldexp(1.0, e - 24);  // FP32 spacing at L
+    return std::fmax(1e-8, 8.0 * ulp);
+}
+
+int pick_device(int& dev, int& nsm) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return fail(SMCRT_ERR_NO_DEVICE, "no CUDA device visible");
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    return SMCRT_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+struct smcrt_ctx {
+    int device = 0, nsm = 0;
+    int precision = SMCRT_FP32, kernel = SMCRT_KERNEL_PATHLENGTH;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Params<float>* pf = nullptr;
+    Params<double>* pd = nullptr;
+    long long ncell = 0, nbins = 0;
+    double* d_jmean = nullptr;
+    double* d_bins = nullptr;
+    unsigned long long* d_work = nullptr;     // [0] work, [1..C_NUM] counters
+    double* d_mom = nullptr;                  // 25
+    int* d_status = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int block = 256, grid_blocks = 0;
+    int timeout_ms = 600000;
+};
+
+namespace {
+
+int occupancy_grid(smcrt_ctx* c, int precision, int kernel, int blocks_per_sm) {
+    int per_sm = 0;
+    cudaError_t e;
+    if (precision == SMCRT_FP64) {
+        e = kernel == SMCRT_KERNEL_WEIGHT ? occupancy_f64_1(c->block, &per_sm)
+            : kernel == SMCRT_KERNEL_TEST ? occupancy_f64_2(c->block, &per_sm)
+                                          : occupancy_f64_0(c->block, &per_sm);
+    } else {
+        e = kernel == SMCRT_KERNEL_WEIGHT ? occupancy_f32_1(c->block, &per_sm)
+            : kernel == SMCRT_KERNEL_TEST ? occupancy_f32_2(c->block, &per_sm)
+                                          : occupancy_f32_0(c->block, &per_sm);
+    }
+    if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
+    if (per_sm < 1) per_sm = 1;
+    if (blocks_per_sm > 0 && blocks_per_sm < per_sm) per_sm = blocks_per_sm;
+    c->grid_blocks = c->nsm * per_sm;
+    return SMCRT_OK;
+}
+
+template <class R>
+Params<R>* make_params(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* src,
+                       const DetT* dets, int ndet, const smcrt_options* o) {
+    Params<R>* P = new Params<R>;
+    std::memset(P, 0, sizeof(*P));
+    fill_scene(P->sc, scene);
+    fill_scene(P->sc64, scene);
+    fill_grid(P->grid, *grid);
+    fill_source(P->src, *src, *grid);
+    for (int i = 0; i < ndet; ++i) P->det[i] = dets[i];
+    P->ndet = ndet;
+    P->kernel = o ? o->kernel : SMCRT_KERNEL_PATHLENGTH;
+    P->end_early = o ? o->end_early : 0;
+    P->max_steps = (o && o->max_trace_steps > 0) ? o->max_trace_steps : 1000000;
+    const int prec = (sizeof(R) == 4) ? SMCRT_FP32 : SMCRT_FP64;
+    P->eps = (R)((o && o->eps > 0) ? o->eps : default_eps(prec, *grid));
+    P->normal_h = (o && o->normal_h > 0) ? o->normal_h : 1e-6;
+    P->instance = o ? o->instance : 0u;
+    P->budget_ns = (unsigned long long)((o && o->timeout_ms > 0) ? o->timeout_ms : 600000) * 1000000ull;
+    return P;
+}
+
+Buffers make_buffers(smcrt_ctx* c, double* jm, double* bins) {
+    Buffers B;
+    B.jmean = jm;
+    B.bins = bins;
+    B.work = c->d_work;
+    B.counters = c->d_work + 1;
+    B.moments = c->d_mom;
+    B.status = c->d_status;
+    B.uniforms = nullptr;
+    B.offsets = nullptr;
+    B.states = nullptr;
+    return B;
+}
+
+int launch_f32(smcrt_ctx* c, const Params<float>& P, const Buffers& B, bool replay, int blocks) {
+    cudaError_t e = P.kernel == SMCRT_KERNEL_WEIGHT ? launch_f32_1(P, B, replay, blocks, c->block, c->stream)
+                    : P.kernel == SMCRT_KERNEL_TEST ? launch_f32_2(P, B, replay, blocks, c->block, c->stream)
+                                                    : launch_f32_0(P, B, replay, blocks, c->block, c->stream);
+    if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    return SMCRT_OK;
+}
+int launch_f64(smcrt_ctx* c, const Params<double>& P, const Buffers& B, bool replay, int blocks) {
+    cudaError_t e = P.kernel == SMCRT_KERNEL_WEIGHT ? launch_f64_1(P, B, replay, blocks, c->block, c->stream)
+                    : P.kernel == SMCRT_KERNEL_TEST ? launch_f64_2(P, B, replay, blocks, c->block, c->stream)
+                                                    : launch_f64_0(P, B, replay, blocks, c->block, c->stream);
+    if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    return SMCRT_OK;
+}
+
+// Enqueues: reset work/counters/status, then the kernel for [first, first+count).
+int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, double* jm, double* bins, bool replay,
+            const double* d_u, const long long* d_off, smcrt_packet_state* d_states) {
+    CK(cudaMemsetAsync(c->d_work, 0, sizeof(unsigned long long) * (1 + C_NUM), c->stream));
+    CK(cudaMemsetAsync(c->d_mom, 0, sizeof(double) * 25, c->stream));
+    CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    Buffers B = make_buffers(c, jm, bins);
+    B.uniforms = d_u;
+    B.offsets = d_off;
+    B.states = d_states;
+    long long need = (count + c->block - 1) / c->block;
+    int blocks = (int)std::min<long long>(c->grid_blocks, std::max<long long>(need, 1));
+    if (c->precision == SMCRT_FP64) {
+        c->pd->first = first;
+        c->pd->count = count;
+        c->pd->seed = seed;
+        return launch_f64(c, *c->pd, B, replay, blocks);
+    }
+    c->pf->first = first;
+    c->pf->count = count;
+    c->pf->seed = seed;
+    return launch_f32(c, *c->pf, B, replay, blocks);
+}
+
+// Waits for ev1.  The kernel enforces the context's time limit itself (a
+// %globaltimer budget, after which threads stop between flights and raise
+// STATUS_ABORTED); the host waits that long plus a grace period.
+int wait_bounded(smcrt_ctx* c) {
+    auto t0 = std::chrono::steady_clock::now();
+    const double limit = (double)c->timeout_ms + 30000.0;
+    for (;;) {
+        cudaError_t e = cudaEventQuery(c->ev1);
+        if (e == cudaSuccess) return SMCRT_OK;
+        if (e != cudaErrorNotReady) return fail(SMCRT_ERR_CUDA, std::string("kernel: ") + cudaGetErrorString(e));
+        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > limit) return fail(SMCRT_ERR_TIMEOUT, "transport kernel did not finish within its time limit");
+        std::this_thread::sleep_for(std::chrono::microseconds(ms < 10 ? 20 : 500));
+    }
+}
+
+int read_stats(smcrt_ctx* c, smcrt_stats* st) {
+    unsigned long long cnt[1 + C_NUM];
+    double mom[25];
+    int status = 0;
+    CK(cudaMemcpy(cnt, c->d_work, sizeof(cnt), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(mom, c->d_mom, sizeof(mom), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    if (st) {
+        std::memset(st, 0, sizeof(*st));
+        const unsigned long long* k = cnt + 1;
+        st->packets = k[C_PACKETS];
+        st->sdf_evals = k[C_SDF];
+        st->voxel_segments = k[C_VOX];
+        st->trace_steps = k[C_STEPS];
+        st->scatters = k[C_SCAT];
+        st->fresnel_events = k[C_FRES];
+        st->reflections = k[C_REFL];
+        st->kills_step_cap = k[C_STEPCAP];
+        st->kills_error = k[C_ERR];
+        st->rng_draws = k[C_DRAWS];
+        for (int i = 0; i < 24; ++i) st->moments[i] = mom[i];
+        st->nscatt = mom[24];
+        st->kernel_ms = ms;
+        st->device_status = status;
+    }
+    if (status & STATUS_ABORTED)
+        return fail(SMCRT_ERR_TIMEOUT, "transport kernel reached its time limit and stopped early");
+    if (status & (STATUS_STREAM_EXHAUSTED | STATUS_BAD_INDEX))
+        return fail(SMCRT_ERR_DEVICE, "device status flag " + std::to_string(status));
+    return SMCRT_OK;
+}
+
+// RAII device buffer for the probes.
+struct DBuf {
+    void* p = nullptr;
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+int upload(DBuf& b, const void* h, size_t bytes) {
+    CK(cudaMalloc(&b.p, bytes ? bytes : 8));
+    if (h && bytes) CK(cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice));
+    return SMCRT_OK;
+}
+
+#define UP(buf, ptr, bytes)                          \
+    do {                                             \
+        int rc_ = upload(buf, ptr, bytes);           \
+        if (rc_) return rc_;                         \
+    } while (0)
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int32_t smcrt_abi_version(void) { return SMCRT_ABI_VERSION; }
+
+const char* smcrt_last_error(void) { return g_err.c_str(); }
+
+int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* source,
+                     const smcrt_detector* dets, int32_t ndet, const smcrt_options* opts, smcrt_ctx** out) {
+    g_err.clear();
+    if (!out) return fail(SMCRT_ERR_ARG, "out is null");
+    *out = nullptr;
+    int rc = validate_scene(scene);
+    if (rc) return rc;
+    rc = validate_optics(scene);
+    if (rc) return rc;
+    if (!grid || grid->nxg <= 0 || grid->nyg <= 0 || grid->nzg <= 0 || !(grid->xmax > 0) || !(grid->ymax > 0) ||
+        !(grid->zmax > 0))
+        return fail(SMCRT_ERR_ARG, "grid: need positive voxel counts and half sizes");
+    if ((long long)grid->nxg * grid->nyg * grid->nzg > (1ll << 31))
+        return fail(SMCRT_ERR_ARG, "grid: more than 2^31 voxels");
+    if (!source || source->kind < SMCRT_SRC_POINT || source->kind > SMCRT_SRC_FOCUS)
+        return fail(SMCRT_ERR_ARG, "source: unknown kind");
+    if (ndet < 0 || ndet > kMaxDetectors || (ndet > 0 && !dets))
+        return fail(SMCRT_ERR_ARG, "detectors: 0.." + std::to_string(kMaxDetectors) + " supported");
+    const int prec = opts ? opts->precision : SMCRT_FP32;
+    const int kern = opts ? opts->kernel : SMCRT_KERNEL_PATHLENGTH;
+    if (prec != SMCRT_FP32 && prec != SMCRT_FP64) return fail(SMCRT_ERR_ARG, "options: unknown precision");
+    if (kern < SMCRT_KERNEL_PATHLENGTH || kern > SMCRT_KERNEL_TEST) return fail(SMCRT_ERR_ARG, "options: unknown kernel");
+    DetT dtab[kMaxDetectors];
+    long long nbins = 0;
+    rc = fill_dets(dtab, dets, ndet, scene->nregions, nbins);
+    if (rc) return rc;
+
+    smcrt_ctx* c = new smcrt_ctx;
+    rc = pick_device(c->device, c->nsm);
+    if (rc) {
+        delete c;
+        return rc;
+    }
+    c->precision = prec;
+    c->kernel = kern;
+    c->ncell = (long long)grid->nxg * grid->nyg * grid->nzg;
+    c->nbins = nbins;
+    c->block = (opts && opts->block_size > 0) ? opts->block_size : 256;
+    if (c->block > 256 || c->block % 32) {
+        delete c;
+        return fail(SMCRT_ERR_ARG, "options: block_size must be a multiple of 32 <= 256");
+    }
+    c->timeout_ms = (opts && opts->timeout_ms > 0) ? opts->timeout_ms : 600000;
+    if (prec == SMCRT_FP64) c->pd = make_params<double>(scene, grid, source, dtab, ndet, opts);
+    else c->pf = make_params<float>(scene, grid, source, dtab, ndet, opts);
+
+    auto bail = [&](int code) {
+        smcrt_destroy(c);
+        return code;
+    };
+#define CKC(call)                                                                                      \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return bail(fail(SMCRT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_))); \
+    } while (0)
+    if (opts && opts->stream) {
+        c->stream = (cudaStream_t)opts->stream;
+    } else {
+        CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    CKC(cudaMalloc(&c->d_jmean, sizeof(double) * c->ncell));
+    CKC(cudaMalloc(&c->d_bins, sizeof(double) * std::max(1ll, nbins)));
+    CKC(cudaMalloc(&c->d_work, sizeof(unsigned long long) * (1 + C_NUM)));
+    CKC(cudaMalloc(&c->d_mom, sizeof(double) * 25));
+    CKC(cudaMalloc(&c->d_status, sizeof(int)));
+    CKC(cudaEventCreate(&c->ev0));
+    CKC(cudaEventCreate(&c->ev1));
+#undef CKC
+    rc = occupancy_grid(c, prec, kern, opts ? opts->blocks_per_sm : 0);
+    if (rc) return bail(rc);
+    *out = c;
+    return SMCRT_OK;
+}
+
+void smcrt_destroy(smcrt_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->d_jmean) cudaFree(c->d_jmean);
+    if (c->d_bins) cudaFree(c->d_bins);
+    if (c->d_work) cudaFree(c->d_work);
+    if (c->d_mom) cudaFree(c->d_mom);
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c->pf;
+    delete c->pd;
+    delete c;
+}
+
+int64_t smcrt_detector_bins(const smcrt_ctx* c) { return c ? c->nbins : -1; }
+
+int32_t smcrt_run_device(smcrt_ctx* c, int64_t first, int64_t count, uint64_t seed, double* jmean_dev,
+                         double* det_bins_dev, smcrt_stats* stats) {
+    g_err.clear();
+    if (!c) return fail(SMCRT_ERR_ARG, "ctx is null");
+    if (first < 0 || count < 0) return fail(SMCRT_ERR_ARG, "negative packet range");
+    if (!jmean_dev || (c->nbins > 0 && !det_bins_dev)) return fail(SMCRT_ERR_ARG, "device buffers are null");
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = enqueue(c, first, count, seed, jmean_dev, det_bins_dev ? det_bins_dev : c->d_bins, false, nullptr,
+                     nullptr, nullptr);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    if (!stats) return SMCRT_OK;
+    rc = wait_bounded(c);
+    if (rc) return rc;
+    return read_stats(c, stats);
+}
+
+int32_t smcrt_run(smcrt_ctx* c, int64_t nphotons, uint64_t seed, double* jmean, double* det_bins,
+                  smcrt_stats* stats) {
+    g_err.clear();
+    if (!c) return fail(SMCRT_ERR_ARG, "ctx is null");
+    if (nphotons < 0) return fail(SMCRT_ERR_ARG, "nphotons < 0");
+    CK(cudaMemsetAsync(c->d_jmean, 0, sizeof(double) * c->ncell, c->stream));
+    CK(cudaMemsetAsync(c->d_bins, 0, sizeof(double) * std::max(1ll, c->nbins), c->stream));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = enqueue(c, 0, nphotons, seed, c->d_jmean, c->d_bins, false, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    rc = wait_bounded(c);
+    if (rc) return rc;
+    if (jmean) CK(cudaMemcpyAsync(jmean, c->d_jmean, sizeof(double) * c->ncell, cudaMemcpyDeviceToHost, c->stream));
+    if (det_bins && c->nbins > 0)
+        CK(cudaMemcpyAsync(det_bins, c->d_bins, sizeof(double) * c->nbins, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return read_stats(c, stats);
+}
+
+int32_t smcrt_replay(smcrt_ctx* c, const double* uniforms, const int64_t* offsets, int64_t npackets, double* jmean,
+                     double* det_bins, smcrt_packet_state* states, smcrt_stats* stats) {
+    g_err.clear();
+    if (!c || !uniforms || !offsets || npackets < 0) return fail(SMCRT_ERR_ARG, "replay: bad arguments");
+    for (int64_t p = 0; p < npackets; ++p)
+        if (offsets[p + 1] < offsets[p]) return fail(SMCRT_ERR_ARG, "replay: offsets must be non-decreasing");
+    const size_t nu = (size_t)offsets[npackets];
+    DBuf du, doff, dst;
+    UP(du, uniforms, sizeof(double) * nu);
+    UP(doff, offsets, sizeof(int64_t) * (npackets + 1));
+    UP(dst, nullptr, sizeof(smcrt_packet_state) * std::max<int64_t>(npackets, 1));
+    CK(cudaMemsetAsync(c->d_jmean, 0, sizeof(double) * c->ncell, c->stream));
+    CK(cudaMemsetAsync(c->d_bins, 0, sizeof(double) * std::max(1ll, c->nbins), c->stream));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = enqueue(c, 0, npackets, 0, c->d_jmean, c->d_bins, true, (const double*)du.p, (const long long*)doff.p,
+                     (smcrt_packet_state*)dst.p);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    rc = wait_bounded(c);
+    if (rc) return rc;
+    if (jmean) CK(cudaMemcpy(jmean, c->d_jmean, sizeof(double) * c->ncell, cudaMemcpyDeviceToHost));
+    if (det_bins && c->nbins > 0) CK(cudaMemcpy(det_bins, c->d_bins, sizeof(double) * c->nbins, cudaMemcpyDeviceToHost));
+    if (states) CK(cudaMemcpy(states, dst.p, sizeof(smcrt_packet_state) * npackets, cudaMemcpyDeviceToHost));
+    return read_stats(c, stats);
+}
+
+int32_t smcrt_run_batched(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* nphotons, const uint64_t* seeds,
+                          double* const* jmeans, double* const* det_bins, smcrt_stats* stats) {
+    g_err.clear();
+    return fail(SMCRT_ERR_ARG, "smcrt_run_batched: not available in this build");
+}
+
+int32_t smcrt_eval_sdf(const smcrt_scene* scene, int32_t precision, const double* pts, int64_t npts, double* out) {
+    g_err.clear();
+    int rc = validate_scene(scene);
+    if (rc) return rc;
+    if (!pts || !out || npts < 0) return fail(SMCRT_ERR_ARG, "eval_sdf: bad arguments");
+    if (npts == 0) return SMCRT_OK;
+    int dev, nsm;
+    rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    DBuf dp, dout;
+    UP(dp, pts, sizeof(double) * 3 * npts);
+    UP(dout, nullptr, sizeof(double) * npts * scene->nregions);
+    CK(probe_eval_sdf(precision, scene, (const double*)dp.p, npts, (double*)dout.p));
+    CK(cudaMemcpy(out, dout.p, sizeof(double) * npts * scene->nregions, cudaMemcpyDeviceToHost));
+    return SMCRT_OK;
+}
+
+int32_t smcrt_calc_normal(const smcrt_scene* scene, int32_t region0, double h, const double* pts, int64_t npts,
+                          double* out) {
+    g_err.clear();
+    int rc = validate_scene(scene);
+    if (rc) return rc;
+    if (region0 < 0 || region0 >= scene->nregions || !pts || !out || npts < 0)
+        return fail(SMCRT_ERR_ARG, "calc_normal: bad arguments");
+    if (npts == 0) return SMCRT_OK;
+    int dev, nsm;
+    rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    DBuf dp, dout;
+    UP(dp, pts, sizeof(double) * 3 * npts);
+    UP(dout, nullptr, sizeof(double) * 3 * npts);
+    CK(probe_normal(scene, region0, h > 0 ? h : 1e-6, (const double*)dp.p, npts, (double*)dout.p));
+    CK(cudaMemcpy(out, dout.p, sizeof(double) * 3 * npts, cudaMemcpyDeviceToHost));
+    return SMCRT_OK;
+}
+
+static int fresnel_common(int32_t precision, const double* I, const double* N, const double* n1, const double* n2,
+                          const double* u, int64_t n, double* R, double* Iout, int32_t* refl) {
+    if (!I || !N || !n1 || !n2 || n < 0) return fail(SMCRT_ERR_ARG, "fresnel: bad arguments");
+    if (n == 0) return SMCRT_OK;
+    int dev, nsm;
+    int rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    DBuf dI, dN, d1, d2, du, dR, dIo, dr;
+    UP(dI, I, sizeof(double) * 3 * n);
+    UP(dN, N, sizeof(double) * 3 * n);
+    UP(d1, n1, sizeof(double) * n);
+    UP(d2, n2, sizeof(double) * n);
+    if (u) {
+        UP(du, u, sizeof(double) * n);
+        UP(dIo, nullptr, sizeof(double) * 3 * n);
+        UP(dr, nullptr, sizeof(int) * n);
+    }
+    if (R) UP(dR, nullptr, sizeof(double) * n);
+    CK(probe_fresnel(precision, (const double*)dI.p, (const double*)dN.p, (const double*)d1.p, (const double*)d2.p,
+                     (const double*)du.p, n, (double*)dR.p, (double*)dIo.p, (int*)dr.p));
+    if (R) CK(cudaMemcpy(R, dR.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (u) {
+        CK(cudaMemcpy(Iout, dIo.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(refl, dr.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    }
+    return SMCRT_OK;
+}
+
+int32_t smcrt_fresnel(int32_t precision, const double* I, const double* N, const double* n1, const double* n2,
+                      int64_t n, double* R) {
+    g_err.clear();
+    if (!R) return fail(SMCRT_ERR_ARG, "fresnel: R is null");
+    return fresnel_common(precision, I, N, n1, n2, nullptr, n, R, nullptr, nullptr);
+}
+
+int32_t smcrt_reflect_refract(int32_t precision, const double* I, const double* N, const double* n1,
+                              const double* n2, const double* u, int64_t n, double* I_out, int32_t* reflected) {
+    g_err.clear();
+    if (!u || !I_out || !reflected) return fail(SMCRT_ERR_ARG, "reflect_refract: bad arguments");
+    return fresnel_common(precision, I, N, n1, n2, u, n, nullptr, I_out, reflected);
+}
+
+int32_t smcrt_scatter_dir(int32_t precision, const double* dir_in, const double* g, const double* u, int64_t n,
+                          double* dir_out) {
+    g_err.clear();
+    if (!dir_in || !g || !u || !dir_out || n < 0) return fail(SMCRT_ERR_ARG, "scatter_dir: bad arguments");
+    if (n == 0) return SMCRT_OK;
+    int dev, nsm;
+    int rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    DBuf dd, dg, du, dout;
+    UP(dd, dir_in, sizeof(double) * 3 * n);
+    UP(dg, g, sizeof(double) * n);
+    UP(du, u, sizeof(double) * 3 * n);
+    UP(dout, nullptr, sizeof(double) * 3 * n);
+    CK(probe_scatter(precision, (const double*)dd.p, (const double*)dg.p, (const double*)du.p, n, (double*)dout.p));
+    CK(cudaMemcpy(dir_out, dout.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+    return SMCRT_OK;
+}
+
+int32_t smcrt_philox(const uint32_t* key2, const uint32_t* ctr4, int64_t n, uint32_t* out4) {
+    g_err.clear();
+    if (!key2 || !ctr4 || !out4 || n < 0) return fail(SMCRT_ERR_ARG, "philox: bad arguments");
+    if (n == 0) return SMCRT_OK;
+    int dev, nsm;
+    int rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    DBuf dk, dc, dout;
+    UP(dk, key2, sizeof(uint32_t) * 2 * n);
+    UP(dc, ctr4, sizeof(uint32_t) * 4 * n);
+    UP(dout, nullptr, sizeof(uint32_t) * 4 * n);
+    CK(probe_philox((const uint32_t*)dk.p, (const uint32_t*)dc.p, n, (uint32_t*)dout.p));
+    CK(cudaMemcpy(out4, dout.p, sizeof(uint32_t) * 4 * n, cudaMemcpyDeviceToHost));
+    return SMCRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,397 @@
+// smcrt_device.cuh -- device building blocks of the B200 photon-packet transport.
+//
+// Everything here is templated on the transport precision R (float or double);
+// boundary events (normal + Fresnel + reflect/refract) always run in double.
+// Reference formulas are cited by file:line of the signedMCRT sources.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/smcrt.h"
+
+namespace smcrt {
+
+constexpr int kMaxPrims = 32;
+constexpr int kMaxRegions = 16;
+constexpr int kMaxDetectors = 16;
+constexpr double kPI = 3.14159265358979323846264338327950288;
+
+// Device status flags (smcrt_stats.device_status).
+enum : int { STATUS_STEP_CAP = 1, STATUS_ERROR_STATE = 2, STATUS_STREAM_EXHAUSTED = 4, STATUS_BAD_INDEX = 8, STATUS_ABORTED = 16 };
+
+// ---------------------------------------------------------------------------
+template <class R>
+struct V3 {
+    R x, y, z;
+};
+template <class R> __host__ __device__ __forceinline__ V3<R> operator+(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class R> __host__ __device__ __forceinline__ V3<R> operator-(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class R> __host__ __device__ __forceinline__ V3<R> operator*(V3<R> a, R s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class R> __host__ __device__ __forceinline__ V3<R> operator*(R s, V3<R> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class R> __device__ __forceinline__ R dot3(V3<R> a, V3<R> b) { return (a.x * b.x) + (a.y * b.y) + (a.z * b.z); }
+template <class R> __device__ __forceinline__ R len3(V3<R> a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+template <class R> __device__ __forceinline__ R clampr(R x, R lo, R hi) { return fmin(fmax(x, lo), hi); }
+template <class R> __device__ __forceinline__ R fsign(R a, R b) { return copysign(fabs(a), b); }  // Fortran sign(a,b)
+__device__ __forceinline__ void sincos_r(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void sincos_r(double x, double* s, double* c) { sincos(x, s, c); }
+__device__ __forceinline__ float cospi_r(float x) { return cospif(x); }
+__device__ __forceinline__ double cospi_r(double x) { return cospi(x); }
+
+// ---------------------------------------------------------------------------
+// Scene tables (kernel-parameter resident: constant bank, warp-broadcast reads).
+template <class R>
+struct DPrim {
+    R m[12];  // row-vector affine, m[3*i+j] = M[i][j]
+    R q[8];
+    int kind;
+    int pad;
+};
+template <class R>
+struct DRegion {
+    int first, n, op, pad;
+    R k, kappa, albedo, hgg, g2, nidx;
+};
+
+template <class R>
+struct SceneT {
+    int nregions, nprims;
+    DPrim<R> prim[kMaxPrims];
+    DRegion<R> region[kMaxRegions];
+};
+
+// pos .dot. transform, src/vector_class.f90:292-304
+template <class R>
+__device__ __forceinline__ V3<R> xform(const R* m, V3<R> a) {
+    V3<R> d;
+    d.x = m[0] * a.x + m[3] * a.y + m[6] * a.z + m[9];
+    d.y = m[1] * a.x + m[4] * a.y + m[7] * a.z + m[10];
+    d.z = m[2] * a.x + m[5] * a.y + m[8] * a.z + m[11];
+    return d;
+}
+
+// Primitive SDFs, src/sdfs/sdfs.f90:494-735
+template <class R>
+__device__ __forceinline__ R eval_prim(const DPrim<R>& pr, V3<R> pos) {
+    const V3<R> p = xform(pr.m, pos);
+    const R* q = pr.q;
+    const R zero = 0, one = 1, half = (R)0.5;
+    switch (pr.kind) {
+        case SMCRT_SPHERE:
+            return sqrt(p.x * p.x + p.y * p.y + p.z * p.z) - q[0];
+        case SMCRT_BOX: {
+            R dx = fabs(p.x) - q[0], dy = fabs(p.y) - q[1], dz = fabs(p.z) - q[2];
+            R mx = fmax(dx, zero), my = fmax(dy, zero), mz = fmax(dz, zero);
+            return sqrt(mx * mx + my * my + mz * mz) + fmin(fmax(dx, fmax(dy, dz)), zero);
+        }
+        case SMCRT_TORUS: {
+            R tx = sqrt(p.x * p.x + zero * zero + p.z * p.z) - q[0];
+            return sqrt(tx * tx + p.y * p.y + zero * zero) - q[1];
+        }
+        case SMCRT_CYLINDER: {
+            V3<R> a{q[0], q[1], q[2]}, b{q[3], q[4], q[5]};
+            V3<R> ba = b - a, pa = p - a;
+            R baba = dot3(ba, ba), paba = dot3(pa, ba);
+            R x = len3(pa * baba - ba * paba) - q[6] * baba;
+            R y = fabs(paba - baba * half) - baba * half;
+            R x2 = x * x, y2 = (y * y) * baba, d;
+            if (fmax(x, y) < zero) {
+                d = -fmin(x2, y2);
+            } else {
+                if (x > zero && y > zero) d = x2 + y2;
+                else if (x > zero) d = x2;
+                else if (y > zero) d = y2;
+                else d = zero;
+            }
+            return fsign(sqrt(fabs(d)) / baba, d);
+        }
+        case SMCRT_TRIPRISM: {
+            return fmax(fabs(p.z) - q[1], fmax(fabs(p.x) * (R)0.866025 + p.y * half, -p.y) - q[0] * half);
+        }
+        case SMCRT_SEGMENT:
+        case SMCRT_CAPSULE: {
+            V3<R> a{q[0], q[1], q[2]}, b{q[3], q[4], q[5]};
+            V3<R> pa = p - a, ba = b - a;
+            R h = clampr(dot3(pa, ba) / dot3(ba, ba), zero, one);
+            R r = (pr.kind == SMCRT_SEGMENT) ? (R)0.1 : q[6];
+            return len3(pa - ba * h) - r;
+        }
+        case SMCRT_CONE: {
+            V3<R> a{q[0], q[1], q[2]}, b{q[3], q[4], q[5]};
+            R ra = q[6], rb = q[7];
+            R rba = rb - ra;
+            R baba = dot3(b - a, b - a);
+            R papa = dot3(p - a, p - a);
+            R paba = dot3(p - a, b - a) / baba;
+            R x = sqrt(fmax(papa - baba * paba * paba, zero));
+            R cax = (paba < half) ? fmax(zero, x - ra) : fmax(zero, x - rb);
+            R cay = fabs(paba - half) - half;
+            R k = rba * rba + baba;
+            R f = clampr((rba * (x - ra) + paba * baba) / k, zero, one);
+            R cbx = x - ra - f * rba;
+            R cby = paba - f;
+            R s = (cbx < zero && cay < zero) ? -one : one;
+            return s * sqrt(fmin(cax * cax + baba * cay * cay, cbx * cbx + baba * cby * cby));
+        }
+        case SMCRT_EGG: {
+            V3<R> pin{fabs(p.x), p.y, p.z};
+            R r = q[0] - q[1];
+            R hin = q[2] + r;
+            R l = (hin * hin - r * r) / ((R)2 * r);
+            if (pin.y <= zero) return len3(pin) - q[0];
+            if ((pin.y - hin) * l > pin.x * hin)
+                return len3(V3<R>{pin.x, pin.y - hin, pin.z}) - ((q[0] + l) - sqrt(hin * hin + l * l));
+            return len3(V3<R>{pin.x + l, pin.y, pin.z}) - (q[0] + l);
+        }
+        case SMCRT_PLANE:
+            return p.x * q[0] + p.y * q[1] + p.z * q[2];
+    }
+    return zero;
+}
+
+// eval_model (src/sdfs/sdf_base.f90:145-160), CSG ops src/sdfs/sdfModifiers.f90:412-475
+template <class R>
+__device__ __forceinline__ R eval_region(const SceneT<R>& sc, int r, V3<R> pos) {
+    const DRegion<R>& g = sc.region[r];
+    R d = eval_prim(sc.prim[g.first], pos);
+    for (int i = 1; i < g.n; ++i) {
+        R d2 = eval_prim(sc.prim[g.first + i], pos);
+        switch (g.op) {
+            case SMCRT_OP_UNION: d = fmin(d, d2); break;
+            case SMCRT_OP_SMOOTH_UNION: {
+                R h = fmax(g.k - fabs(d - d2), (R)0) / g.k;
+                d = fmin(d, d2) - h * h * h * g.k * ((R)1 / (R)6);
+                break;
+            }
+            case SMCRT_OP_SUBTRACTION: d = fmax(-d, d2); break;
+            case SMCRT_OP_INTERSECTION: d = fmax(d, d2); break;
+        }
+    }
+    return d;
+}
+
+// calcNormal, src/sdfs/sdf_base.f90:165-189 (always double)
+__device__ __forceinline__ V3<double> calc_normal(const SceneT<double>& sc, int r, V3<double> p, double h) {
+    const V3<double> xyy{1, -1, -1}, yyx{-1, -1, 1}, yxy{-1, 1, -1}, xxx{1, 1, 1};
+    V3<double> n = xyy * eval_region(sc, r, p + xyy * h) + yyx * eval_region(sc, r, p + yyx * h) +
+                   yxy * eval_region(sc, r, p + yxy * h) + xxx * eval_region(sc, r, p + xxx * h);
+    double t = len3(n);
+    return V3<double>{n.x / t, n.y / t, n.z / t};
+}
+
+// fresnel / reflect / refract, src/surfaces.f90:42-120
+template <class R>
+__device__ __forceinline__ R fresnel(V3<R> I, V3<R> N, R n1, R n2) {
+    R costt = fabs(dot3(I, N));
+    R sintt = sqrt((R)1 - costt * costt);
+    R sint2 = n1 / n2 * sintt;
+    if (sint2 > (R)1) return (R)1;
+    if (costt == (R)1) return (R)0;
+    R cost2 = sqrt((R)1 - sint2 * sint2);
+    R f1 = fabs((n1 * costt - n2 * cost2) / (n1 * costt + n2 * cost2));
+    R f2 = fabs((n1 * cost2 - n2 * costt) / (n1 * cost2 + n2 * costt));
+    return (R)0.5 * (f1 * f1 + f2 * f2);
+}
+template <class R>
+__device__ __forceinline__ V3<R> reflect(V3<R> I, V3<R> N) {
+    return I - (R)2 * dot3(N, I) * N;
+}
+template <class R>
+__device__ __forceinline__ V3<R> refract(V3<R> I, V3<R> N, R eta) {
+    V3<R> Nt = N;
+    R c1 = dot3(Nt, I);
+    if (c1 < (R)0) c1 = -c1;
+    else Nt = (R)(-1) * N;
+    R c2 = sqrt((R)1 - (eta * eta) * ((R)1 - c1 * c1));
+    return eta * I + (eta * c1 - c2) * Nt;
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11).
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t c2,
+                                                       uint32_t c3, uint32_t out[4]) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+template <class R> struct U01;
+template <> struct U01<float> {
+    static constexpr int kWords = 1;
+    __device__ __forceinline__ static float from(uint32_t a, uint32_t) { return (float)(a >> 9) * 0x1p-23f + 0x1p-24f; }
+};
+template <> struct U01<double> {
+    static constexpr int kWords = 2;
+    __device__ __forceinline__ static double from(uint32_t a, uint32_t b) {
+        uint64_t m = ((uint64_t)a << 20) | (uint64_t)(b >> 12);
+        return (double)m * 0x1p-52 + 0x1p-53;
+    }
+};
+
+// Per-packet uniform stream: counter RNG keyed (seed, instance, packet id), or
+// an injected stream (replay mode).
+// Per-packet uniform stream: counter RNG keyed (seed, instance, packet id); in
+// replay builds (INJ) an injected uniform stream instead.
+template <class R, bool INJ = false>
+struct Stream {
+    uint32_t k0, k1, inst, p0, p1, block;
+    uint32_t b0, b1, b2, b3;  // unconsumed Philox words, consumed from b0 (register queue)
+    int left;
+    int ndraws;
+    const double* inj;
+    int ninj;
+    int flags;
+
+    __device__ __forceinline__ void init(uint64_t seed, uint32_t instance, uint64_t pid, const double* injected, int n) {
+        k0 = (uint32_t)seed;
+        k1 = (uint32_t)(seed >> 32);
+        inst = instance;
+        p0 = (uint32_t)pid;
+        p1 = (uint32_t)(pid >> 32);
+        block = 0;
+        left = 0;
+        ndraws = 0;
+        inj = injected;
+        ninj = n;
+        flags = 0;
+    }
+    __device__ __forceinline__ R next() {
+        if (INJ) {
+            if (ndraws >= ninj) {
+                flags |= STATUS_STREAM_EXHAUSTED;
+                ++ndraws;
+                return (R)0.5;
+            }
+            return (R)inj[ndraws++];
+        }
+        if (left < U01<R>::kWords) {
+            uint32_t o[4];
+            philox4x32_10(k0, k1, block, inst, p0, p1, o);
+            b0 = o[0];
+            b1 = o[1];
+            b2 = o[2];
+            b3 = o[3];
+            ++block;
+            left = 4;
+        }
+        R u;
+        if (U01<R>::kWords == 1) {
+            u = U01<R>::from(b0, 0u);
+            b0 = b1;
+            b1 = b2;
+            b2 = b3;
+        } else {
+            u = U01<R>::from(b0, b1);
+            b0 = b2;
+            b1 = b3;
+        }
+        left -= U01<R>::kWords;
+        ++ndraws;
+        return u;
+    }
+};
+
+// scatter, src/photon.f90:713-779 (the bias test with p = 0 consumes one draw when g != 0)
+template <class R, class Rng>
+__device__ __forceinline__ V3<R> hg_scatter(V3<R> d, R hgg, R g2, Rng& rng) {
+    const R one = 1, two = 2;
+    R cost;
+    if (hgg == (R)0) {
+        cost = two * rng.next() - one;
+    } else {
+        (void)rng.next();
+        R temp = (one - g2) / (one - hgg + two * hgg * rng.next());
+        cost = (one + g2 - temp * temp) / (two * hgg);
+    }
+    R sint = sqrt(one - cost * cost);
+    R u = rng.next();
+    const R cosp = cospi_r(two * u);  // cos(2 pi u)
+    R sabs = sqrt(one - cosp * cosp);
+    R sinp = (u < (R)0.5) ? sabs : -sabs;  // phi < pi  <=>  u < 1/2
+    bool vertical = (one - fabs(d.z) <= (R)1e-12);
+    R temp = 0;
+    if (!vertical) {
+        temp = (sizeof(R) == 4) ? sqrt(d.x * d.x + d.y * d.y) : sqrt(one - d.z * d.z);
+        if (temp == (R)0) vertical = true;
+    }
+    V3<R> o;
+    if (vertical) {
+        o.x = sint * cosp;
+        o.y = sint * sinp;
+        o.z = fsign(cost, d.z);
+    } else {
+        o.x = sint * (d.x * d.z * cosp - d.y * sinp) / temp + d.x * cost;
+        o.y = sint * (d.y * d.z * cosp + d.x * sinp) / temp + d.y * cost;
+        o.z = -one * sint * cosp * temp + d.z * cost;
+    }
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// Grid and detectors.
+template <class R>
+struct GridT {
+    int nx, ny, nz, pad;
+    R xmax, ymax, zmax;
+    R vx, vy, vz;       // voxel sizes 2*max/n
+    R sx, sy, sz;       // n/(2*max) as written: n * p / (2 * max)
+    double xmax_d, ymax_d, zmax_d;  // exact half sizes (grid-exit test on FP64 positions)
+};
+
+struct DetT {
+    int kind, layer, nb, pad;  // nb = bins per axis (nbins + 1)
+    long long off;
+    double pos[3], dir[3];
+    double r1, r2, bw, bwy;
+    double e1[3], e2[3], n[3], width, height;
+};
+
+template <class R>
+struct SourceT {
+    int kind, annulus_type;
+    R pos[3], dir[3], p1[3], p2[3], p3[3];
+    R radius, radius_hi, sin_beta, cos_beta, zstart;
+    R rot[9];  // circular source rotation (rotationAlign), row-major M[i][j]
+    int circ_swap;
+};
+
+// Launch parameters (one __grid_constant__ block in the constant bank).
+template <class R>
+struct Params {
+    SceneT<R> sc;
+    SceneT<double> sc64;  // boundary events
+    GridT<R> grid;
+    SourceT<R> src;
+    DetT det[kMaxDetectors];
+    int ndet;
+    int kernel;
+    int end_early;
+    int max_steps;
+    R eps;
+    double normal_h;
+    unsigned long long seed;
+    unsigned long long budget_ns;  // per-launch device time budget (0 = none)
+    unsigned int instance;
+    long long first;
+    long long count;
+};
+
+}  // namespace smcrt

@@ -1,0 +1,37 @@
+// smcrt_launch.h -- host-side entry points of the separately compiled kernel
+// variants (one translation unit per transport precision x kernel kind, built
+// from smcrt_kernels.cu with -DSMCRT_R/-DSMCRT_TAG/-DSMCRT_K).
+#pragma once
+
+#include "smcrt_transport.cuh"
+
+namespace smcrt {
+
+#define SMCRT_DECL_VARIANT(R, TAG, K)                                                                       \
+    cudaError_t launch_##TAG##_##K(const Params<R>& P, const Buffers& B, bool replay, int blocks, int block, \
+                                   cudaStream_t s);                                                       \
+    cudaError_t occupancy_##TAG##_##K(int block, int* per_sm);
+
+SMCRT_DECL_VARIANT(float, f32, 0)
+SMCRT_DECL_VARIANT(float, f32, 1)
+SMCRT_DECL_VARIANT(float, f32, 2)
+SMCRT_DECL_VARIANT(double, f64, 0)
+SMCRT_DECL_VARIANT(double, f64, 1)
+SMCRT_DECL_VARIANT(double, f64, 2)
+#undef SMCRT_DECL_VARIANT
+
+// Device-function probes (smcrt_probes.cu).
+cudaError_t probe_eval_sdf(int precision, const smcrt_scene* scene, const double* d_pts, long long n, double* d_out);
+cudaError_t probe_normal(const smcrt_scene* scene, int region, double h, const double* d_pts, long long n,
+                         double* d_out);
+cudaError_t probe_fresnel(int precision, const double* I, const double* N, const double* n1, const double* n2,
+                          const double* u, long long n, double* R_out, double* I_out, int* refl);
+cudaError_t probe_scatter(int precision, const double* dir, const double* g, const double* u, long long n,
+                          double* out);
+cudaError_t probe_philox(const uint32_t* key, const uint32_t* ctr, long long n, uint32_t* out);
+
+// Scene conversion shared by the API and the probes.
+template <class R>
+void fill_scene(SceneT<R>& d, const smcrt_scene* s);
+
+}  // namespace smcrt

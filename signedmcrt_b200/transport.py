@@ -1,0 +1,184 @@
+"""Python view of the C ABI: one `Transport` per simulation (smcrt_create), with
+host-buffer runs (smcrt_run), device-resident runs (smcrt_run_device, e.g. into
+torch tensors), stream replay (smcrt_replay) and batched runs.
+
+Fluence arrays come back as (nxg, nyg, nzg) float64 views in Fortran order, so
+`jmean[i-1, j-1, k-1]` is the reference's `jmean(i, j, k)`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from ._lib import check, lib
+from .config import Settings
+from .scene import FlatScene
+
+KERNELS = {"pathlength": abi.KERNEL_PATHLENGTH, "weight": abi.KERNEL_WEIGHT, "test": abi.KERNEL_TEST}
+PRECISIONS = {"fp32": abi.FP32, "fp64": abi.FP64}
+
+
+@dataclass
+class RunResult:
+    jmean: np.ndarray | None      # (nxg, nyg, nzg) float64, Fortran order
+    bins: np.ndarray | None       # concatenated detector bins
+    stats: dict
+
+    @property
+    def nscatt(self) -> float:
+        return self.stats["nscatt"]
+
+
+class Transport:
+    def __init__(self, array, settings: Settings, *, kernel: str = "pathlength", precision: str = "fp32",
+                 end_early: bool = False, stream: int | None = None, block_size: int = 0, blocks_per_sm: int = 0,
+                 eps: float = 0.0, normal_h: float = 0.0, max_trace_steps: int = 0, timeout_ms: int = 0,
+                 instance: int = 0):
+        self.settings = settings
+        self.flat = array if isinstance(array, FlatScene) else FlatScene(array)
+        self.grid = settings.grid_c()
+        self.source = settings.source_c()
+        dets = settings.detectors_c()
+        self._dets = (abi.Detector * max(1, len(dets)))(*dets)
+        self.ndet = len(dets)
+        o = abi.Options()
+        o.kernel = KERNELS[kernel]
+        o.precision = PRECISIONS[precision]
+        o.end_early = int(bool(end_early))
+        o.block_size, o.blocks_per_sm = block_size, blocks_per_sm
+        o.max_trace_steps = max_trace_steps
+        o.eps, o.normal_h = eps, normal_h
+        o.instance = instance
+        o.timeout_ms = timeout_ms
+        o.stream = stream
+        self.options = o
+        self.kernel, self.precision = kernel, precision
+        self._ctx = C.c_void_p()
+        check(lib().smcrt_create(self.flat.ptr(), C.byref(self.grid), C.byref(self.source), self._dets,
+                                 self.ndet, C.byref(o), C.byref(self._ctx)))
+        self.nbins = int(lib().smcrt_detector_bins(self._ctx))
+        g = settings.grid
+        self.shape = (g.nxg, g.nyg, g.nzg)
+        self.ncell = g.nxg * g.nyg * g.nzg
+
+    # ------------------------------------------------------------------
+    def close(self) -> None:
+        if self._ctx:
+            lib().smcrt_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _grid_view(self, flat: np.ndarray) -> np.ndarray:
+        return flat.reshape(self.shape, order="F")
+
+    # ------------------------------------------------------------------
+    def run(self, nphotons: int, seed: int, *, jmean_out: np.ndarray | None = None,
+            bins_out: np.ndarray | None = None, want_jmean: bool = True) -> RunResult:
+        """Packets [0, nphotons) of stream `seed`; tallies copied to host buffers
+        (pass pinned buffers as jmean_out/bins_out to reuse them)."""
+        jm = None
+        if want_jmean:
+            jm = jmean_out if jmean_out is not None else np.empty(self.ncell, dtype=np.float64)
+        bins = bins_out if bins_out is not None else np.zeros(max(self.nbins, 0), dtype=np.float64)
+        st = abi.Stats()
+        check(lib().smcrt_run(self._ctx, int(nphotons), int(seed), abi.dptr(jm),
+                              abi.dptr(bins) if self.nbins else None, C.byref(st)))
+        return RunResult(self._grid_view(jm) if jm is not None else None, bins, st.to_dict())
+
+    def run_device(self, first: int, count: int, seed: int, jmean_dev: int, bins_dev: int | None,
+                   stats: bool = False) -> dict | None:
+        """Adds the tallies of packets [first, first+count) into caller-owned device
+        buffers (raw pointers, e.g. tensor.data_ptr()), asynchronously on the
+        context stream; with stats=True it synchronises and returns counters."""
+        st = abi.Stats() if stats else None
+        check(lib().smcrt_run_device(self._ctx, int(first), int(count), int(seed), C.c_void_p(jmean_dev),
+                                     C.c_void_p(bins_dev) if bins_dev else None,
+                                     C.byref(st) if st is not None else None))
+        return st.to_dict() if st is not None else None
+
+    def replay(self, uniforms: np.ndarray, offsets: np.ndarray):
+        """Runs packets from injected uniform streams; returns (RunResult, states)."""
+        uniforms = np.ascontiguousarray(uniforms, dtype=np.float64)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        n = len(offsets) - 1
+        jm = np.empty(self.ncell, dtype=np.float64)
+        bins = np.zeros(max(self.nbins, 0), dtype=np.float64)
+        states = np.zeros(max(n, 1), dtype=abi.PACKET_STATE_DTYPE)
+        st = abi.Stats()
+        check(lib().smcrt_replay(self._ctx, abi.dptr(uniforms), abi.i64ptr(offsets), n, abi.dptr(jm),
+                                 abi.dptr(bins) if self.nbins else None, states.ctypes.data_as(C.c_void_p),
+                                 C.byref(st)))
+        return RunResult(self._grid_view(jm), bins, st.to_dict()), states[:n]
+
+
+# ---------------------------------------------------------------------- probes
+def eval_sdf(flat: FlatScene, pts: np.ndarray, precision: str = "fp32") -> np.ndarray:
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    out = np.empty((len(pts), flat.nregions), dtype=np.float64)
+    check(lib().smcrt_eval_sdf(flat.ptr(), PRECISIONS[precision], abi.dptr(pts), len(pts), abi.dptr(out)))
+    return out
+
+
+def calc_normal(flat: FlatScene, region0: int, pts: np.ndarray, h: float = 1e-6) -> np.ndarray:
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    out = np.empty_like(pts)
+    check(lib().smcrt_calc_normal(flat.ptr(), region0, h, abi.dptr(pts), len(pts), abi.dptr(out)))
+    return out
+
+
+def fresnel(I, N, n1, n2, precision: str = "fp32") -> np.ndarray:
+    I = np.ascontiguousarray(I, dtype=np.float64).reshape(-1, 3)
+    N = np.ascontiguousarray(N, dtype=np.float64).reshape(-1, 3)
+    n1 = np.ascontiguousarray(np.broadcast_to(n1, len(I)), dtype=np.float64)
+    n2 = np.ascontiguousarray(np.broadcast_to(n2, len(I)), dtype=np.float64)
+    R = np.empty(len(I), dtype=np.float64)
+    check(lib().smcrt_fresnel(PRECISIONS[precision], abi.dptr(I), abi.dptr(N), abi.dptr(n1), abi.dptr(n2),
+                              len(I), abi.dptr(R)))
+    return R
+
+
+def reflect_refract(I, N, n1, n2, u, precision: str = "fp32"):
+    I = np.ascontiguousarray(I, dtype=np.float64).reshape(-1, 3)
+    N = np.ascontiguousarray(N, dtype=np.float64).reshape(-1, 3)
+    n = len(I)
+    n1 = np.ascontiguousarray(np.broadcast_to(n1, n), dtype=np.float64)
+    n2 = np.ascontiguousarray(np.broadcast_to(n2, n), dtype=np.float64)
+    u = np.ascontiguousarray(np.broadcast_to(u, n), dtype=np.float64)
+    out = np.empty_like(I)
+    refl = np.empty(n, dtype=np.int32)
+    check(lib().smcrt_reflect_refract(PRECISIONS[precision], abi.dptr(I), abi.dptr(N), abi.dptr(n1),
+                                      abi.dptr(n2), abi.dptr(u), n, abi.dptr(out), abi.i32ptr(refl)))
+    return out, refl.astype(bool)
+
+
+def scatter_dir(dirs, g, u, precision: str = "fp32") -> np.ndarray:
+    dirs = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+    n = len(dirs)
+    g = np.ascontiguousarray(np.broadcast_to(g, n), dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(n, 3)
+    out = np.empty_like(dirs)
+    check(lib().smcrt_scatter_dir(PRECISIONS[precision], abi.dptr(dirs), abi.dptr(g), abi.dptr(u), n,
+                                  abi.dptr(out)))
+    return out
+
+
+def philox(key: np.ndarray, ctr: np.ndarray) -> np.ndarray:
+    key = np.ascontiguousarray(key, dtype=np.uint32).reshape(-1, 2)
+    ctr = np.ascontiguousarray(ctr, dtype=np.uint32).reshape(-1, 4)
+    out = np.empty_like(ctr)
+    check(lib().smcrt_philox(abi.u32ptr(key), abi.u32ptr(ctr), len(ctr), abi.u32ptr(out)))
+    return out
