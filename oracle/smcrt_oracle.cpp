@@ -400,6 +400,7 @@ struct Packet {
 struct Pol {
     double eps, delta, h;
     bool ref_dda, crossing_f64;
+    bool kill_le;  // device semantics: d <= eps at the start of a flight counts as on the surface
     int64_t max_steps;
 };
 
@@ -585,7 +586,9 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
         R dsdf = std::numeric_limits<R>::infinity();
         for (int i = 0; i < N; ++i) dsdf = std::min(dsdf, std::fabs(eval_region(sc, i, cv<R>(pos))));
         c.sdf += N;
-        if (dsdf < eps) {
+        // reference: kill if d < eps (inttau2.f90:58); device semantics also kills
+        // at d == eps, where the trace loop (d > eps, :63) has already stopped
+        if (pol.kill_le ? dsdf <= eps : dsdf < eps) {
             pk.tflag = true;
             break;
         }
@@ -712,23 +715,56 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
     if (std::fabs(pos.z) > g.zmax) pk.tflag = true;
 }
 
-// scatter, src/photon.f90:713-779 (bias test p = 0 consumes one draw when g != 0)
+// scatter, src/photon.f90:713-779 (bias test p = 0 consumes one draw when g != 0).
+// FP64: the reference's formulas.  FP32 (device semantics): the same angles from
+// forms free of 1 - cos^2 cancellation -- 1 -+ cos(theta) factored out of the HG
+// inverse CDF, and sin/cos(phi) of 2 pi u evaluated accurately.
+inline void hg_angles(float hgg, float g2, float u, float& cost, float& sint) {
+    float omc, opc;
+    if (hgg == 0.0f) {
+        omc = 2.0f * (1.0f - u);
+        opc = 2.0f * u;
+    } else {
+        const float den = 1.0f - hgg + 2.0f * hgg * u;
+        const float temp = (1.0f - g2) / den;
+        omc = (1.0f - hgg) * (1.0f - u) * (temp + (1.0f - hgg)) / den;
+        opc = (1.0f + hgg) * u * (1.0f + hgg + temp) / den;
+    }
+    cost = (omc < opc) ? 1.0f - omc : opc - 1.0f;
+    sint = std::sqrt(omc * opc);
+}
+inline void hg_angles(double hgg, double g2, double u, double& cost, double& sint) {
+    if (hgg == 0.0) {
+        cost = 2.0 * u - 1.0;
+    } else {
+        const double temp = (1.0 - g2) / (1.0 - hgg + 2.0 * hgg * u);
+        cost = (1.0 + g2 - temp * temp) / (2.0 * hgg);
+    }
+    sint = std::sqrt(1.0 - cost * cost);
+}
+inline void phi_angles(float u, float& cosp, float& sinp) {
+    const double a = 2.0 * kPI * (double)u;
+    cosp = (float)std::cos(a);
+    sinp = (float)std::sin(a);
+}
+inline void phi_angles(double u, double& cosp, double& sinp) {
+    const double phi = (2.0 * kPI) * u;
+    cosp = std::cos(phi);
+    sinp = (phi < kPI) ? std::sqrt(1.0 - cosp * cosp) : -std::sqrt(1.0 - cosp * cosp);
+}
+
 template <class R, class Rng>
 void scatter(V3<R>& dir, R hgg, R g2, Rng& rng) {
-    const R one = 1, two = 2;
-    const R TWOPI = (R)(2.0 * kPI), PI = (R)kPI;
-    R cost;
+    const R one = 1;
+    R cost, sint;
     if (hgg == (R)0) {
-        cost = two * rng.next() - one;
+        hg_angles(hgg, g2, rng.next(), cost, sint);
     } else {
         (void)rng.next();  // ran2() < p with p = 0 (:739)
-        R temp = (one - g2) / (one - hgg + two * hgg * rng.next());
-        cost = (one + g2 - temp * temp) / (two * hgg);
+        hg_angles(hgg, g2, rng.next(), cost, sint);
     }
-    R sint = std::sqrt(one - cost * cost);
-    R phi = TWOPI * rng.next();
-    R cosp = std::cos(phi);
-    R sinp = (phi < PI) ? std::sqrt(one - cosp * cosp) : -std::sqrt(one - cosp * cosp);
+    R cosp, sinp;
+    phi_angles(rng.next(), cosp, sinp);
     R uxx, uyy, uzz;
     R nx = dir.x, ny = dir.y, nz = dir.z;
     bool vertical = (one - std::fabs(nz) <= (R)1e-12);
@@ -772,8 +808,9 @@ void emit(const smcrt_source& s, const GridD& g, Packet<R>& pk, Rng& rng) {
             ep = opos;
             R phi = rng.next() * TWOPI;
             R cosp = std::cos(phi), sinp = std::sin(phi);
-            R cost = (R)2 * rng.next() - (R)1;
-            R sint = std::sqrt((R)1 - cost * cost);
+            R u2 = rng.next();
+            R cost = (R)2 * u2 - (R)1;
+            R sint = (sizeof(R) == 4) ? (R)2 * std::sqrt(u2 * ((R)1 - u2)) : std::sqrt((R)1 - cost * cost);
             pk.dir = V3<R>{sint * cosp, sint * sinp, cost};
             break;
         }
@@ -1157,6 +1194,7 @@ int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt
     A.pol.h = pol->normal_h;
     A.pol.ref_dda = pol->ref_dda != 0;
     A.pol.crossing_f64 = pol->crossing_f64 != 0;
+    A.pol.kill_le = pol->ref_dda == 0;  // device semantics
     A.pol.max_steps = pol->max_trace_steps > 0 ? pol->max_trace_steps : 1000000;
     A.first = first;
     A.count = count;

@@ -49,8 +49,11 @@ def _units() -> list[tuple[Path, list[str]]]:
     units = []
     for rtype, tag, k in VARIANTS:
         obj = BUILD / f"kernels_{tag}_{k}.o"
-        units.append((obj, ["-DSMCRT_R=" + rtype, "-DSMCRT_TAG=" + tag, f"-DSMCRT_K={k}",
-                            "-c", str(CSRC / "smcrt_kernels.cu"), "-o", str(obj)]))
+        # the FP64 variants are the accuracy mode: no FMA contraction, so their
+        # arithmetic follows the CPU restatement operation for operation
+        fmad = ["--fmad=false"] if tag == "f64" else []
+        units.append((obj, fmad + ["-DSMCRT_R=" + rtype, "-DSMCRT_TAG=" + tag, f"-DSMCRT_K={k}",
+                                   "-c", str(CSRC / "smcrt_kernels.cu"), "-o", str(obj)]))
     for name in ("smcrt_probes", "smcrt_api"):
         obj = BUILD / f"{name}.o"
         units.append((obj, ["-c", str(CSRC / f"{name}.cu"), "-o", str(obj)]))

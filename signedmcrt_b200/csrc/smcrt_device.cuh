@@ -309,23 +309,53 @@ struct Stream {
     }
 };
 
-// scatter, src/photon.f90:713-779 (the bias test with p = 0 consumes one draw when g != 0)
+// scatter, src/photon.f90:713-779 (the bias test with p = 0 consumes one draw
+// when g != 0).  FP64 uses the reference's formulas; FP32 evaluates the same
+// angles in forms free of the 1 - cos^2 cancellations: 1 -+ cos(theta) come
+// factored out of the HG inverse CDF, and sin/cos(phi) from sincospi, so the
+// FP32 direction is accurate to a few ulps even for near-forward scatters.
+__device__ __forceinline__ void hg_angles(float hgg, float g2, float u, float& cost, float& sint) {
+    float omc, opc;  // 1 - cos(theta), 1 + cos(theta)
+    if (hgg == 0.0f) {
+        omc = 2.0f * (1.0f - u);
+        opc = 2.0f * u;
+    } else {
+        const float den = 1.0f - hgg + 2.0f * hgg * u;
+        const float temp = (1.0f - g2) / den;
+        omc = (1.0f - hgg) * (1.0f - u) * (temp + (1.0f - hgg)) / den;
+        opc = (1.0f + hgg) * u * (1.0f + hgg + temp) / den;
+    }
+    cost = (omc < opc) ? 1.0f - omc : opc - 1.0f;
+    sint = sqrtf(omc * opc);
+}
+__device__ __forceinline__ void hg_angles(double hgg, double g2, double u, double& cost, double& sint) {
+    if (hgg == 0.0) {
+        cost = 2.0 * u - 1.0;
+    } else {
+        const double temp = (1.0 - g2) / (1.0 - hgg + 2.0 * hgg * u);
+        cost = (1.0 + g2 - temp * temp) / (2.0 * hgg);
+    }
+    sint = sqrt(1.0 - cost * cost);
+}
+__device__ __forceinline__ void phi_angles(float u, float& cosp, float& sinp) { sincospif(2.0f * u, &sinp, &cosp); }
+__device__ __forceinline__ void phi_angles(double u, double& cosp, double& sinp) {
+    cosp = cospi(2.0 * u);
+    const double s = sqrt(1.0 - cosp * cosp);
+    sinp = (u < 0.5) ? s : -s;  // phi = 2 pi u < pi  <=>  u < 1/2
+}
+
 template <class R, class Rng>
 __device__ __forceinline__ V3<R> hg_scatter(V3<R> d, R hgg, R g2, Rng& rng) {
-    const R one = 1, two = 2;
-    R cost;
+    const R one = 1;
+    R cost, sint;
     if (hgg == (R)0) {
-        cost = two * rng.next() - one;
+        hg_angles(hgg, g2, rng.next(), cost, sint);
     } else {
         (void)rng.next();
-        R temp = (one - g2) / (one - hgg + two * hgg * rng.next());
-        cost = (one + g2 - temp * temp) / (two * hgg);
+        hg_angles(hgg, g2, rng.next(), cost, sint);
     }
-    R sint = sqrt(one - cost * cost);
-    R u = rng.next();
-    const R cosp = cospi_r(two * u);  // cos(2 pi u)
-    R sabs = sqrt(one - cosp * cosp);
-    R sinp = (u < (R)0.5) ? sabs : -sabs;  // phi < pi  <=>  u < 1/2
+    R cosp, sinp;
+    phi_angles(rng.next(), cosp, sinp);
     bool vertical = (one - fabs(d.z) <= (R)1e-12);
     R temp = 0;
     if (!vertical) {

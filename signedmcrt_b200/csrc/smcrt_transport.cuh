@@ -134,7 +134,10 @@ __device__ __forceinline__ void tauint2(const Params<R>& P, double* __restrict__
             for (int i = 0; i < N; ++i) dsdf = fmin(dsdf, fabs(eval_region(sc, i, pf)));
         }
         c.sdf += N;
-        if (dsdf < eps) {
+        // The reference kills here when d < eps and stops tracing when d <= eps
+        // (inttau2.f90:58,63); a packet left at d == eps (reachable on the FP32
+        // coordinate grid) is treated as on the surface, like a reflected packet.
+        if (dsdf <= eps) {
             pk.tflag = true;
             break;
         }
@@ -276,8 +279,10 @@ __device__ __forceinline__ void emit(const Params<R>& P, Pk<R>& pk, Rng& rng) {
             const R phi = rng.next() * TWOPI;
             R sp, cp;
             sincos_r(phi, &sp, &cp);
-            const R cost = (R)2 * rng.next() - (R)1;
-            const R sint = sqrt((R)1 - cost * cost);
+            const R u2 = rng.next();
+            const R cost = (R)2 * u2 - (R)1;
+            // FP32: sin(theta) = 2 sqrt(u (1 - u)), free of the 1 - cos^2 cancellation
+            const R sint = (sizeof(R) == 4) ? (R)2 * sqrt(u2 * ((R)1 - u2)) : sqrt((R)1 - cost * cost);
             pk.dir = V3<R>{sint * cp, sint * sp, cost};
             break;
         }

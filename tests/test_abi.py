@@ -1,0 +1,92 @@
+"""The C-ABI boundary without a GPU: the library loads, exports every function
+include/smcrt.h declares, and the ctypes mirror has the header's struct layout."""
+import ctypes as C
+import json
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from signedmcrt_b200 import abi
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "smcrt.h"
+
+
+def declared_functions(header: Path = HEADER) -> list[str]:
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:[\w\*\s]+?)\b(smcrt_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_header_declares_expected_entry_points():
+    names = declared_functions()
+    for must in ("smcrt_create", "smcrt_run", "smcrt_run_device", "smcrt_replay", "smcrt_run_batched",
+                 "smcrt_destroy", "smcrt_last_error", "smcrt_eval_sdf", "smcrt_calc_normal", "smcrt_fresnel"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from signedmcrt_b200 import _lib
+    if not _lib.LIB_PATH.exists():
+        from signedmcrt_b200 import build
+        build.build()
+    lib = C.CDLL(str(_lib.LIB_PATH))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(abi.SIGNATURES) <= set(declared_functions())
+    abi.bind(lib)
+    assert lib.smcrt_abi_version() == abi.ABI_VERSION
+
+
+def test_no_device_is_an_error_not_a_crash():
+    """Without a visible GPU, creation reports SMCRT_ERR_NO_DEVICE (or succeeds on a GPU host)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    from signedmcrt_b200 import _lib, presets as P, transport as T
+    st = P.benchmark_settings("box_slab")
+    with pytest.raises(_lib.SmcrtError) as e:
+        T.Transport(P.setup_simulation(st), st)
+    assert e.value.code == abi.ERR_NO_DEVICE
+
+
+STRUCTS = {
+    "smcrt_prim": (abi.Prim, ["kind", "transform", "params"]),
+    "smcrt_region": (abi.Region, ["first_prim", "nprims", "op", "layer_id", "k", "mus", "mua", "hgg", "n"]),
+    "smcrt_scene": (abi.Scene, ["nregions", "nprims", "regions", "prims"]),
+    "smcrt_grid": (abi.Grid, ["nxg", "nyg", "nzg", "xmax", "ymax", "zmax"]),
+    "smcrt_source": (abi.Source, ["kind", "annulus_type", "pos", "dir", "point1", "point2", "point3", "radius",
+                                  "radius_hi", "beta", "z_inset"]),
+    "smcrt_detector": (abi.Detector, ["kind", "layer", "nbins", "pos", "dir", "r1", "r2", "maxval", "p2", "p3"]),
+    "smcrt_options": (abi.Options, ["kernel", "precision", "end_early", "block_size", "blocks_per_sm",
+                                    "max_trace_steps", "eps", "normal_h", "instance", "timeout_ms", "stream"]),
+    "smcrt_stats": (abi.Stats, ["nscatt", "packets", "sdf_evals", "voxel_segments", "trace_steps", "scatters",
+                                "fresnel_events", "reflections", "kills_step_cap", "kills_error", "rng_draws",
+                                "moments", "kernel_ms", "device_status"]),
+    "smcrt_packet_state": (abi.PacketState, ["pos", "dir", "weight", "layer", "nscatt", "ndraws", "flags"]),
+}
+
+
+def test_struct_layout_matches_header(tmp_path):
+    """Compiles a C probe against include/smcrt.h and compares sizes/offsets with ctypes."""
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "smcrt.h"', "int main(void){", 'printf("{");']
+    first = True
+    for name, (_, fields) in STRUCTS.items():
+        sep = "" if first else ","
+        first = False
+        lines.append(f'printf("{sep}\\"{name}\\":{{\\"size\\":%zu", sizeof({name}));')
+        for f in fields:
+            lines.append(f'printf(",\\"{f}\\":%zu", offsetof({name}, {f}));')
+        lines.append('printf("}");')
+    lines += ['printf("}\\n");', "return 0;}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    layout = json.loads(subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout)
+    for name, (cls, fields) in STRUCTS.items():
+        assert C.sizeof(cls) == layout[name]["size"], name
+        for f in fields:
+            assert getattr(cls, f).offset == layout[name][f], (name, f)

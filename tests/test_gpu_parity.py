@@ -1,0 +1,367 @@
+"""GPU parity: the sm_100a path through the C ABI against the CPU oracle.
+
+(a) building blocks (SDF values, normals, Fresnel, reflect/refract, HG scatter,
+    Philox) -- FP32 within 1e-5 (relative to max(1, |value|)), FP64 to rounding;
+(b) per-packet histories replayed from injected uniform streams -- FP64 identical
+    to the oracle's device semantics, FP32 within 1e-5 of the reference semantics;
+(c) whole runs on the counter RNG -- FP64 event counters identical to the oracle,
+    FP32 fluence and detector totals statistically equal (chi-square per voxel
+    block, totals within 3 sigma) to the reference-semantics oracle.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from signedmcrt_b200 import abi, presets as P, scene as S
+from tests import reference_kats as K
+from tests.test_oracle_kats import make_prim, scat_test2_settings, scat_test_settings
+
+pytestmark = pytest.mark.gpu
+OPT0 = S.mono(0.0, 0.0, 0.0, 0.0)
+TOL32 = 1e-5
+
+
+def fluence_agrees(a, b, rtol_voxel=1e-6):
+    """FP64 tallies of the same histories: total to 1e-12, 10^3-voxel blocks to 1e-7,
+    and at least 99.9% of voxels to rtol_voxel.  Individual voxels may differ more
+    where a ~1e-9 position difference (libm ulps amplified along a long history)
+    moves a voxel-face crossing."""
+    assert abs(a.sum() - b.sum()) <= 1e-12 * abs(b.sum())
+    ba, bb = block_sums(a), block_sums(b)
+    assert np.allclose(ba, bb, rtol=1e-7, atol=1e-10 * bb.max())
+    bad = np.abs(a - b) > rtol_voxel * np.abs(b) + 1e-12 * b.max()
+    assert bad.mean() <= 1e-3, bad.sum()
+
+
+def all_primitives_scene():
+    arr = [make_prim(name, args) for name, args, _ in K.SDF_KATS]
+    t = S.invert(S.translate((0.1, -0.2, 0.3))) @ np.eye(4)
+    arr.append(S.box((1.0, 0.5, 0.8), OPT0, 1, transform=S.invert(S.rotate_y(30.0)) @ S.invert(S.translate((0.2, 0, 0)))))
+    arr.append(S.capsule((-0.5, 0, 0), (0.5, 0.2, 0), 0.3, OPT0, 1, transform=t))
+    kids = [S.sphere(0.25, OPT0, 1), S.box((1.0, 1.0, 1.0), OPT0, 1)]
+    for op in (S.union, S.smooth_union, S.subtraction, S.intersection):
+        arr.append(S.model(kids, op, 0.1))
+    return S.FlatScene(arr[:16])
+
+
+def test_sdf_values(gpu, oracle):
+    flat = all_primitives_scene()
+    rng = np.random.default_rng(0)
+    pts = np.concatenate([rng.uniform(-3, 3, (4000, 3)), rng.uniform(-0.3, 0.3, (1000, 3))])
+    ref = oracle.eval_sdf(flat, pts, "fp64")
+    g64 = gpu.eval_sdf(flat, pts, "fp64")
+    g32 = gpu.eval_sdf(flat, pts, "fp32")
+    assert np.allclose(g64, ref, rtol=0, atol=1e-13)
+    assert np.all(np.abs(g32 - ref) <= TOL32 * np.maximum(1.0, np.abs(ref)))
+
+
+def test_sdf_known_answers_on_device(gpu):
+    for name, args, cases in K.SDF_KATS:
+        flat = S.FlatScene([make_prim(name, args)])
+        pts = np.array([c[0] for c in cases], dtype=np.float64)
+        got = gpu.eval_sdf(flat, pts, "fp64")[:, 0]
+        for (p, want, thr), g in zip(cases, got):
+            assert abs(g - want) <= (thr if thr is not None else 4e-16), (name, p, g)
+
+
+def test_normals(gpu, oracle):
+    flat = all_primitives_scene()
+    rng = np.random.default_rng(1)
+    pts = rng.uniform(-1.5, 1.5, (500, 3))
+    for r in range(flat.nregions):
+        a = gpu.calc_normal(flat, r, pts)
+        b = oracle.calc_normal(flat, r, pts)
+        ok = np.isfinite(b).all(axis=1)
+        assert np.allclose(a[ok], b[ok], atol=1e-9), r
+    sph = S.FlatScene([S.sphere(1.0, OPT0, 1)])
+    for p, n in K.NORMAL_KATS:
+        assert np.allclose(gpu.calc_normal(sph, 0, [p])[0], n, atol=1e-9)
+
+
+def random_incidence(n, seed):
+    rng = np.random.default_rng(seed)
+    I = rng.normal(size=(n, 3))
+    I /= np.linalg.norm(I, axis=1, keepdims=True)
+    N = rng.normal(size=(n, 3))
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    n1 = rng.choice([1.0, 1.33, 1.38, 1.45], n)
+    n2 = rng.choice([1.0, 1.33, 1.36, 1.4], n)
+    return I, N, n1, n2
+
+
+def well_conditioned(I, N, n1, n2, margin=0.05):
+    """Away from the critical angle, where R and the refracted direction have
+    unbounded sensitivity to cos(theta): the transmitted cos^2 = 1 - sin^2 must
+    exceed `margin` (or total internal reflection must hold by that margin)."""
+    c = np.abs(np.einsum("ij,ij->i", I, N))
+    s2 = n1 / n2 * np.sqrt(np.maximum(0.0, 1 - c * c))
+    return np.abs(1.0 - s2 * s2) > margin
+
+
+def test_fresnel_and_reflect_refract(gpu, oracle):
+    """The transport evaluates boundary events in FP64 (identical to the oracle);
+    the FP32 form of the same functions is checked on well-conditioned inputs."""
+    I, N, n1, n2 = random_incidence(20000, 2)
+    ok = well_conditioned(I, N, n1, n2)
+    assert ok.mean() > 0.85
+    R64 = oracle.fresnel(I, N, n1, n2)
+    assert np.allclose(gpu.fresnel(I, N, n1, n2, "fp64"), R64, atol=1e-14)
+    assert np.all(np.abs(gpu.fresnel(I, N, n1, n2, "fp32") - R64)[ok] <= TOL32)
+    u = np.random.default_rng(3).random(len(I))
+    o64, r64 = oracle.reflect_refract(I, N, n1, n2, u)
+    g64, gr64 = gpu.reflect_refract(I, N, n1, n2, u, "fp64")
+    assert np.array_equal(r64, gr64) and np.allclose(g64, o64, atol=1e-13)
+    g32, gr32 = gpu.reflect_refract(I, N, n1, n2, u, "fp32")
+    same = (gr32 == r64) & ok   # a draw within FP32 rounding of R may fall either side
+    assert same.mean() > 0.85
+    assert np.all(np.abs(g32[same] - o64[same]) <= TOL32)
+    # normal incidence and total internal reflection (surfaces.f90:104-109)
+    Ik = np.array([[0, 0, -1.0], [math.sin(1.2), 0, math.cos(1.2)]])
+    Nk = np.array([[0, 0, 1.0], [0, 0, 1.0]])
+    for prec in ("fp32", "fp64"):
+        Rk = gpu.fresnel(Ik, Nk, np.array([1.0, 1.45]), np.array([1.33, 1.0]), prec)
+        assert Rk[0] == 0.0 and Rk[1] == 1.0
+
+
+def test_hg_scatter(gpu, oracle):
+    rng = np.random.default_rng(4)
+    n = 20000
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d[:50] = (0, 0, 1.0)
+    d[50:100] = (0, 0, -1.0)
+    g = rng.choice([0.0, 0.8, 0.9, 0.85], n)
+    u = rng.random((n, 3))
+    ref = oracle.scatter_dir(d, g, u, "fp64")
+    assert np.allclose(gpu.scatter_dir(d, g, u, "fp64"), ref, atol=1e-13)
+    assert np.all(np.abs(gpu.scatter_dir(d, g, u, "fp32") - ref) <= TOL32)
+
+
+def test_philox_on_device(gpu):
+    for key, ctr, want in K.PHILOX_KATS:
+        assert tuple(int(x) for x in gpu.philox(key, ctr)[0]) == want
+    rng = np.random.default_rng(5)
+    key = rng.integers(0, 2**32, (1000, 2), dtype=np.uint64).astype(np.uint32)
+    ctr = rng.integers(0, 2**32, (1000, 4), dtype=np.uint64).astype(np.uint32)
+    from oracle import binding
+    assert np.array_equal(gpu.philox(key, ctr), binding.philox(key, ctr))
+
+
+# ---------------------------------------------------------------- replay
+SCENES = ["box_slab", "sphere_water", "layered_vessels"]
+
+
+def streams(npk, per, seed):
+    u = np.random.default_rng(seed).random(npk * per)
+    u = np.where(u == 0.0, 0.5, u)
+    return u, np.arange(0, npk * per + 1, per, dtype=np.int64)
+
+
+@pytest.mark.parametrize("cfg", SCENES)
+def test_replay_fp64_matches_oracle(gpu, oracle, cfg):
+    """FP64 replay: every discrete decision identical to the oracle (draw count,
+    scatter count, final layer, detector bins); positions agree to 1e-9 after
+    tens of boundary events (libm-ulp differences amplified by curved refraction)."""
+    st = P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+    u, off = streams(512, 6000, 11)
+    with gpu.Transport(arr, st, precision="fp64") as tr:
+        res, states = tr.replay(u, off)
+    ref = oracle.run(arr, st, nphotons=512, seed=0, policy=oracle.device_policy("fp64", st.grid_c()),
+                     uniforms=u, offsets=off, want_states=True)
+    assert not np.any(states["flags"] & 4), "a packet exhausted its stream"
+    assert np.array_equal(states["layer"], ref.states["layer"])
+    assert np.array_equal(states["nscatt"], ref.states["nscatt"])
+    assert np.array_equal(states["ndraws"], ref.states["ndraws"])
+    assert np.allclose(states["pos"], ref.states["pos"], atol=1e-9)
+    assert np.allclose(states["dir"], ref.states["dir"], atol=1e-9)
+    fluence_agrees(res.jmean, ref.jmean)
+    assert np.array_equal(res.bins, ref.bins)
+
+
+def short_history(cfg):
+    """The scene with absorbing optics (mua = max(mua, mus)): about two interactions
+    per packet, so one history is a well-conditioned function of its stream."""
+    st = P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+
+    def absorb(o):
+        return S.mono(o.mus, max(o.mua, o.mus), o.hgg, o.n)
+    out = []
+    for ent in arr:
+        if isinstance(ent, S.Model):
+            for k in ent.children:
+                k.opt = absorb(k.opt)
+        else:
+            ent.opt = absorb(ent.opt)
+        out.append(ent)
+    return out, st
+
+
+def history_close(a, b, tol=TOL32):
+    same = (a["ndraws"] == b["ndraws"]) & (a["layer"] == b["layer"]) & (a["nscatt"] == b["nscatt"])
+    return same & np.all(np.abs(a["pos"] - b["pos"]) <= tol * np.maximum(1, np.abs(b["pos"])), axis=1) \
+        & np.all(np.abs(a["dir"] - b["dir"]) <= 10 * tol, axis=1)
+
+
+@pytest.mark.parametrize("cfg", SCENES)
+def test_replay_fp32_single_histories_within_1e5(gpu, oracle, cfg):
+    """FP32 histories replayed from the same uniforms as the FP64 reference algorithm
+    end within 1e-5 (positions, cm scale) of it.  A history may differ only where a
+    discrete decision lands within rounding of its threshold."""
+    arr, st = short_history(cfg)
+    u, off = streams(4096, 400, 12)
+    with gpu.Transport(arr, st, precision="fp32") as tr:
+        _, states = tr.replay(u, off)
+    ref = oracle.run(arr, st, nphotons=4096, seed=0, policy=oracle.reference_policy(), uniforms=u, offsets=off,
+                     want_states=True, want_jmean=False)
+    assert not np.any(states["flags"] & 4)
+    assert history_close(states, ref.states).mean() >= 0.99
+
+
+@pytest.mark.parametrize("cfg", SCENES)
+def test_replay_fp32_full_scenes_track_oracle(gpu, oracle, cfg):
+    """Full-length FP32 histories (tens of events) against the oracle's FP32 device
+    semantics: the large majority stay within 1e-5; the rest diverge through
+    ulp-level differences (FMA, libm) amplified at curved refracting surfaces."""
+    st = P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+    u, off = streams(1024, 6000, 13)
+    with gpu.Transport(arr, st, precision="fp32") as tr:
+        _, states = tr.replay(u, off)
+    ref = oracle.run(arr, st, nphotons=1024, seed=0, policy=oracle.device_policy("fp32", st.grid_c()),
+                     uniforms=u, offsets=off, want_states=True, want_jmean=False)
+    assert history_close(states, ref.states).mean() >= 0.9
+
+
+# ---------------------------------------------------------------- counter RNG runs
+COUNT_KEYS = ("nscatt", "sdf_evals", "voxel_segments", "trace_steps", "scatters", "fresnel_events", "reflections",
+              "rng_draws", "kills_error", "kills_step_cap")
+
+
+@pytest.mark.parametrize("cfg", SCENES)
+@pytest.mark.parametrize("kernel", ["pathlength", "weight"])
+def test_fp64_run_matches_oracle_exactly(gpu, oracle, cfg, kernel):
+    st = P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+    n = 20000
+    with gpu.Transport(arr, st, precision="fp64", kernel=kernel) as tr:
+        g = tr.run(n, 99)
+    o = oracle.run(arr, st, nphotons=n, seed=99, kernel=kernel, policy=oracle.device_policy("fp64", st.grid_c()))
+    diff = {k: (g.stats[k], o.stats[k]) for k in COUNT_KEYS if g.stats[k] != o.stats[k]}
+    assert not diff, diff
+    fluence_agrees(g.jmean, o.jmean)
+    assert np.array_equal(g.bins, o.bins)
+
+
+def block_sums(j, b=10):
+    nx, ny, nz = j.shape
+    return j.reshape(nx // b, b, ny // b, b, nz // b, b).sum(axis=(1, 3, 5))
+
+
+@pytest.mark.parametrize("cfg,n_or,batches,bsz", [("box_slab", 200000, 32, 100000),
+                                                  ("layered_vessels", 100000, 32, 50000)])
+def test_fp32_fluence_statistical_parity(gpu, oracle, cfg, n_or, batches, bsz):
+    """FP32 GPU fluence vs the reference-semantics FP64 oracle on independent seeds:
+    chi-square over 10^3-voxel blocks and the total path length within 3 sigma."""
+    st = P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+    o = oracle.run(arr, st, nphotons=n_or, seed=424242, policy=oracle.reference_policy())
+    ob = block_sums(o.jmean) / n_or
+    sums, sq, bins = 0.0, 0.0, []
+    tot = []
+    with gpu.Transport(arr, st, precision="fp32") as tr:
+        for b in range(batches):
+            r = tr.run(bsz, 1000 + b)
+            m = block_sums(r.jmean) / bsz
+            sums = sums + m
+            sq = sq + m * m
+            tot.append(r.jmean.sum() / bsz)
+            bins.append(r.bins / bsz)
+    mg = sums / batches
+    var_pp = (sq / batches - mg * mg) * batches / (batches - 1) * bsz  # per-packet variance
+    ng = batches * bsz
+    se = np.sqrt(var_pp / ng + var_pp / n_or)
+    mask = (mg > 1e-3 * mg.max()) & (se > 0)
+    z = (mg[mask] - ob[mask]) / se[mask]
+    dof = mask.sum()
+    chi2 = float((z * z).sum())
+    assert dof > 50
+    assert chi2 / dof < 1 + 5 * math.sqrt(2 / dof), (chi2, dof)
+    tot = np.array(tot)
+    se_tot = tot.std(ddof=1) * math.sqrt(bsz) * math.sqrt(1 / ng + 1 / n_or)
+    assert abs(tot.mean() - o.jmean.sum() / n_or) <= 3 * se_tot
+    if st.detectors:
+        bins = np.array(bins)
+        gb, obn = bins.mean(axis=0), o.bins / n_or
+        seb = bins.std(axis=0, ddof=1) * math.sqrt(bsz) * math.sqrt(1 / ng + 1 / n_or)
+        ok = seb > 0
+        assert np.all(np.abs(gb - obn)[ok] <= 4 * seb[ok])
+        assert abs(gb.sum() - obn.sum()) <= 3 * math.sqrt((seb ** 2).sum())
+
+
+def test_scatter_test1_on_device(gpu):
+    st = scat_test_settings()
+    with gpu.Transport(P.setup_simulation(st), st, kernel="test") as tr:
+        r = tr.run(100000, 123456789)
+    assert abs(r.nscatt / 1e5 - K.SCAT_TEST1_NSCATT) <= K.SCAT_TEST1_THR
+
+
+def test_scatter_test2_on_device(gpu):
+    st = scat_test2_settings()
+    N = 10_000_000
+    with gpu.Transport(P.setup_simulation(st), st, kernel="test", end_early=True) as tr:
+        r = tr.run(N, 123456789, want_jmean=False)
+    m = r.stats["moments"]
+    got = np.concatenate([10.0 * m[:12].reshape(4, 3), 100.0 * m[12:].reshape(4, 3)]) / N
+    for row, want in zip(got, K.SCAT_TEST2_MOMENTS):
+        for ax in range(3):
+            assert abs(row[ax] - want[ax]) <= K.SCAT_TEST2_THR[ax], (row, want)
+
+
+def test_run_device_into_torch_tensors_equals_run(gpu):
+    import torch
+    st = P.benchmark_settings("layered_vessels")
+    arr = P.setup_simulation(st)
+    with gpu.Transport(arr, st, precision="fp64") as tr:
+        ref = tr.run(30000, 5)
+        jm = torch.zeros(tr.ncell, dtype=torch.float64, device="cuda")
+        bins = torch.zeros(tr.nbins, dtype=torch.float64, device="cuda")
+        # two shards of the packet range add up to the whole run
+        tr.run_device(0, 10000, 5, jm.data_ptr(), bins.data_ptr())
+        tr.run_device(10000, 20000, 5, jm.data_ptr(), bins.data_ptr(), stats=True)
+    got = jm.cpu().numpy().reshape(tr.shape, order="F")
+    assert np.allclose(got, ref.jmean, rtol=1e-11, atol=1e-12 * ref.jmean.max())
+    assert np.array_equal(bins.cpu().numpy(), ref.bins)
+
+
+def test_time_budget_stops_the_kernel_and_context_stays_usable(gpu):
+    """A run past its time limit returns SMCRT_ERR_TIMEOUT (device-side budget, no
+    fault) and the same context runs normally afterwards."""
+    from signedmcrt_b200 import _lib
+    st = P.benchmark_settings("sphere_water")
+    arr = P.setup_simulation(st)
+    with gpu.Transport(arr, st, timeout_ms=20) as tr:
+        with pytest.raises(_lib.SmcrtError) as e:
+            tr.run(2_000_000_000, 1)
+        assert e.value.code == abi.ERR_TIMEOUT
+        r = tr.run(1000, 2)
+        assert r.stats["packets"] == 1000 and r.stats["device_status"] == 0
+
+
+def test_invalid_inputs_are_errors(gpu):
+    from signedmcrt_b200 import _lib
+    st = P.benchmark_settings("box_slab")
+    bad = [S.box((2, 2, 2), S.mono(-1.0, 0.1, 0.9, 1.38), 1)]
+    with pytest.raises(_lib.SmcrtError) as e:
+        gpu.Transport(bad, st)
+    assert e.value.code == abi.ERR_SCENE
+    too_many = [S.sphere(0.1 * (i + 1), S.mono(1, 0, 0, 1), i) for i in range(40)]
+    with pytest.raises(_lib.SmcrtError) as e:
+        gpu.Transport(too_many, st)
+    assert e.value.code == abi.ERR_SCENE
+    st.grid.nxg = 0
+    with pytest.raises(_lib.SmcrtError) as e:
+        gpu.Transport(P.setup_simulation(st), st)
+    assert e.value.code == abi.ERR_ARG
