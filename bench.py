@@ -1,0 +1,341 @@
+"""Benchmark: photon packets/s of the transport path on the curved-surface
+refraction workload (sphere r=1 cm in a 4 cm water box, top-hat beam, 200^3
+FP64 fluence grid, 1e8 packets per step), one rank per GPU.
+
+A step is one full pass of the packet loop over the workload's packets,
+starting from a zeroed tally grid.  Ranks take disjoint packet-id ranges of the
+same counter-based RNG stream (weak scaling: each rank runs the full per-GPU
+packet count) and their FP64 tallies are summed onto rank 0 with one NCCL
+reduce, which is part of the step.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints ONE JSON line on rank 0.  `value` is device-resident throughput timed
+with CUDA events on the launch stream; `e2e` goes through the C ABI's host-buffer
+entry point (smcrt_run) with pinned host tallies copied back every step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "photon packets/s at matched fluence RMS error"
+UNIT = "packets/s"
+
+# Algorithmic FP32 work per counted event (flop, FMA = 2), from the source
+# formulas: affine transform of a point = 9 FMA + 3 add; primitive bodies below;
+# one voxel segment = 1 compare-select + face/dir divide + FP64 tally add; one
+# trace step = optical-depth update + compare + position advance; one HG
+# scatter = inverse CDF + rotation (3 sqrt, 1 sincospi).  Boundary events run in
+# FP64 and are counted as their 4 SDF evaluations plus 60 flop.
+XFORM_FLOP = 21
+PRIM_FLOP = {1: 8, 2: 20, 3: 16, 4: 45, 5: 14, 6: 25, 7: 27, 8: 50, 9: 30, 10: 5}
+VOXEL_FLOP, STEP_FLOP, SCATTER_FLOP, FRESNEL_FLOP = 12, 10, 35, 60
+TALLY_BYTES = 16  # one FP64 read-modify-write per voxel segment
+
+
+def peaks() -> dict:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured", "sm_max_mhz": d.get("sm_max_mhz", 1965.0)}
+    return {"hbm_gbs": 6650.0, "source": "fallback", "sm_max_mhz": 1965.0}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[4:8]) if v.strip().lower() == "active"})
+        power = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(power) if power else None}
+
+
+def algorithmic_work(stats: dict, flat) -> tuple[float, float]:
+    """(flop, bytes) of the reference algorithm for the counted events."""
+    regions = flat.c.regions
+    prims = flat.c.prims
+    per_region = []
+    for i in range(flat.nregions):
+        r = regions[i]
+        per_region.append(sum(XFORM_FLOP + PRIM_FLOP[prims[r.first_prim + j].kind] for j in range(r.nprims)))
+    w_sdf = sum(per_region) / len(per_region)
+    flop = (w_sdf * stats["sdf_evals"] + VOXEL_FLOP * stats["voxel_segments"] + STEP_FLOP * stats["trace_steps"] +
+            SCATTER_FLOP * stats["scatters"] + FRESNEL_FLOP * stats["fresnel_events"])
+    nbytes = TALLY_BYTES * stats["voxel_segments"]
+    return flop, nbytes
+
+
+def cpu_baseline(arr, st, target_s: float, threads: int = 0) -> dict:
+    """The oracle's reference-semantics path (FP64, OpenMP over packets, all host
+    threads) on a bounded sample of the same workload."""
+    from oracle import binding as O
+    pol = O.reference_policy(threads=threads, tally_f32=True)
+    n = 20000
+    t = time.perf_counter()
+    O.run(arr, st, nphotons=n, seed=9001, policy=pol)
+    dt = time.perf_counter() - t
+    n2 = int(min(max(n * target_s / max(dt, 1e-3), 20000), 5e7))
+    t = time.perf_counter()
+    O.run(arr, st, nphotons=n2, seed=9002, policy=pol)
+    dt2 = time.perf_counter() - t
+    cores = threads or O.max_threads()
+    return {"value": n2 / dt2, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n2} packets of the workload, reference semantics (FP64, eps 1e-8, snapping voxel walk, "
+                      f"FP32 atomic tally as the reference), {cores} OpenMP threads, {dt2:.1f} s"}
+
+
+def run_reference(args, arr, st, workload: dict) -> None:
+    """`--impl reference`: the oracle's restatement of the reference's CPU path, timed
+    on the host cores; rank 0 only."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import binding as O
+    pol = O.reference_policy(tally_f32=True)
+    cores = O.max_threads()
+    t = time.perf_counter()
+    O.run(arr, st, nphotons=10000, seed=1, policy=pol)
+    rate = 10000 / max(time.perf_counter() - t, 1e-3)
+    n = int(min(max(rate * args.ref_step_s, 10000), 5e7))
+    for w in range(args.warmup):
+        O.run(arr, st, nphotons=max(n // 10, 1000), seed=100 + w, policy=pol)
+    times = []
+    for k in range(args.steps):
+        t = time.perf_counter()
+        O.run(arr, st, nphotons=n, seed=200 + k, policy=pol)
+        times.append(time.perf_counter() - t)
+    value = n * len(times) / sum(times)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload, packets_per_step=n,
+                           note="each step is a bounded sample of the workload on the host cores"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{n} packets per step, reference semantics (FP64, OpenMP over packets)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="sphere_water", choices=["sphere_water", "box_slab", "layered_vessels"])
+    ap.add_argument("--packets", type=float, default=0, help="packets per GPU per step (default: the config's)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ref-step-s", type=float, default=8.0, help="reference arm: seconds of CPU work per step")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours" and not args.packets:
+        print("note: fewer than 3 warm-up steps", file=sys.stderr)
+
+    from signedmcrt_b200 import presets as P
+    from signedmcrt_b200.scene import FlatScene
+    st = P.benchmark_settings(args.config)
+    arr = P.setup_simulation(st)
+    flat = FlatScene(arr)
+    per_gpu = int(args.packets) if args.packets else int(st.source.nphotons)
+    g = st.grid
+    workload = {"workload": f"{args.config}: " + {
+        "sphere_water": "sphere r=1 cm (mua .05, mus 50, g .85, n 1.45) in a 4 cm water box, top-hat r=0.5 cm",
+        "box_slab": "2 cm box (mua .1, mus 10, g .9, n 1.38), pencil beam",
+        "layered_vessels": "3 layers + 4 capsule vessels, pencil beam, 10 annular detectors"}[args.config],
+        "grid": [g.nxg, g.nyg, g.nzg], "tally": "fp64", "packets_per_gpu_per_step": per_gpu}
+
+    if args.impl == "reference":
+        run_reference(args, arr, st, workload)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from signedmcrt_b200 import transport as T
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)  # every timed launch goes to this stream
+    torch.cuda.set_stream(stream)
+    tr = T.Transport(flat, st, precision=args.precision, stream=stream.cuda_stream, timeout_ms=600000)
+    jm = torch.zeros(tr.ncell, dtype=torch.float64, device=dev)
+    bins = torch.zeros(max(tr.nbins, 1), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    first = rank * per_gpu
+    seed = st.simulation.iseed
+
+    def step(k: int, evs=None):
+        flush.zero_()
+        jm.zero_()
+        bins.zero_()
+        if evs is not None:
+            evs[0].record(stream)
+        tr.run_device(first, per_gpu, seed + k, jm.data_ptr(), bins.data_ptr() if tr.nbins else None)
+        if evs is not None:
+            evs[1].record(stream)
+        if world > 1:
+            dist.reduce(jm, 0)
+            if tr.nbins:
+                dist.reduce(bins, 0)
+
+    for w in range(args.warmup):
+        step(1000 + w)
+    torch.cuda.synchronize(dev)
+    # event counters of one step (same kernel, counters always on)
+    stats = tr.run_device(first, per_gpu, seed + 999, jm.data_ptr(), bins.data_ptr() if tr.nbins else None,
+                          stats=True)
+
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev.index if dev.index is not None else 0) as clk:
+        t0.record(stream)
+        for k in range(args.steps):
+            step(k, kev[k])
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    kern_ms = [a.elapsed_time(b) for a, b in kev]
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * per_gpu * args.steps / (ms / 1e3)
+
+    # e2e through the C ABI (host buffers, pinned), same packets per step
+    e2e = None
+    if not args.no_e2e:
+        jh = torch.empty(tr.ncell, dtype=torch.float64, pin_memory=True).numpy()
+        bh = torch.empty(max(tr.nbins, 1), dtype=torch.float64, pin_memory=True).numpy()
+        tr_host = T.Transport(flat, st, precision=args.precision, timeout_ms=600000)
+        tr_host.run(min(per_gpu, 100000), 1, jmean_out=jh, bins_out=bh[:tr_host.nbins] if tr_host.nbins else None)
+        if world > 1:
+            dist.barrier()
+        times = []
+        for k in range(args.steps):
+            t = time.perf_counter()
+            tr_host.run(per_gpu, seed + 500 + k, jmean_out=jh, bins_out=bh[:tr_host.nbins] if tr_host.nbins else None)
+            times.append(time.perf_counter() - t)
+        tr_host.close()
+        e_ms = 1e3 * sum(times) / len(times)
+        if world > 1:
+            t = torch.tensor([e_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": world * per_gpu / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": 0,  # inputs are the scene tables and a packet range, passed as kernel params
+               "d2h_bytes_per_step": 8 * (tr.ncell + tr.nbins), "ms_per_step": e_ms,
+               "path": "smcrt_run (C ABI, pinned host tallies, blocking)"}
+
+    if rank == 0:
+        pk = peaks()
+        flop, nbytes = algorithmic_work(stats, flat)
+        kmean = sum(kern_ms) / len(kern_ms)
+        achieved_gbs = nbytes / (kmean / 1e3) / 1e9
+        clocks = clk.summary()
+        mhz = clocks.get("sm_mhz") or pk["sm_max_mhz"]
+        fp32_peak = 148 * 128 * 2 * (pk["sm_max_mhz"] * 1e6) / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+            "config": dict(workload, parallelism=f"packet-range shards x{world}, NCCL reduce of FP64 tallies",
+                           l2="flushed between steps (256 MiB write)", precision=args.precision,
+                           rng="Philox4x32-10 keyed (seed, packet id)"),
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None,
+                         "peak_source": pk["source"],
+                         "bytes_per_packet": nbytes / stats["packets"],
+                         "kernel_ms": kmean,
+                         "fp32_issue": {"achieved_tflops": flop / (kmean / 1e3) / 1e12,
+                                        "peak_tflops": fp32_peak, "frac": flop / (kmean / 1e3) / 1e12 / fp32_peak,
+                                        "peak_source": "nominal 148 SM x 128 lanes x 2 x max SM clock",
+                                        "flop_per_packet": flop / stats["packets"]},
+                         "events_per_packet": {k: stats[k] / stats["packets"] for k in
+                                               ("sdf_evals", "voxel_segments", "trace_steps", "scatters",
+                                                "fresnel_events", "rng_draws")}},
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+        }
+        if e2e is not None:
+            line["e2e"] = e2e
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(arr, st, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    tr.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -170,8 +170,11 @@ typedef struct smcrt_options {
     double normal_h;       /* finite-difference step of the normal; <= 0 -> 1e-6
                               (sdf_base.f90:176); normals are evaluated in FP64 */
     uint32_t instance;     /* RNG stream id (second counter word) */
-    int32_t timeout_ms;    /* host wait limit for smcrt_run; 0 = 600000 */
-    void* stream;          /* cudaStream_t to launch on; NULL = a stream owned by ctx */
+    int32_t timeout_ms;    /* time limit of one run in ms (device-side budget); 0 = 600000 */
+    void* stream;          /* cudaStream_t to launch on; NULL = the default stream */
+    int32_t private_stream;/* nonzero: the context creates and owns a non-blocking stream
+                              and ignores `stream` */
+    int32_t reserved2;
 } smcrt_options;
 
 /* Event counters of one run (definitions identical in the CPU oracle). */

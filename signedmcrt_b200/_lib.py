@@ -7,7 +7,10 @@ from pathlib import Path
 
 from . import abi
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libsmcrt_b200.so"
+import os
+
+# SMCRT_B200_LIB selects another build of the same library (e.g. a tuned variant)
+LIB_PATH = Path(os.environ.get("SMCRT_B200_LIB", Path(__file__).resolve().parent / "lib" / "libsmcrt_b200.so"))
 
 _lib: C.CDLL | None = None
 

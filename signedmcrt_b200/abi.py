@@ -66,7 +66,8 @@ class Options(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("precision", C.c_int32), ("end_early", C.c_int32),
                 ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("max_trace_steps", C.c_int32),
                 ("eps", C.c_double), ("normal_h", C.c_double), ("instance", C.c_uint32),
-                ("timeout_ms", C.c_int32), ("stream", C.c_void_p)]
+                ("timeout_ms", C.c_int32), ("stream", C.c_void_p), ("private_stream", C.c_int32),
+                ("reserved2", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -442,11 +442,11 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
         cudaError_t e_ = (call);                                                                       \
         if (e_ != cudaSuccess) return bail(fail(SMCRT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_))); \
     } while (0)
-    if (opts && opts->stream) {
-        c->stream = (cudaStream_t)opts->stream;
-    } else {
+    if (opts && opts->private_stream) {
         CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         c->own_stream = true;
+    } else {
+        c->stream = opts ? (cudaStream_t)opts->stream : (cudaStream_t)0;
     }
     CKC(cudaMalloc(&c->d_jmean, sizeof(double) * c->ncell));
     CKC(cudaMalloc(&c->d_bins, sizeof(double) * std::max(1ll, nbins)));
@@ -464,7 +464,7 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
 
 void smcrt_destroy(smcrt_ctx* c) {
     if (!c) return;
-    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->stream);
     if (c->d_jmean) cudaFree(c->d_jmean);
     if (c->d_bins) cudaFree(c->d_bins);
     if (c->d_work) cudaFree(c->d_work);

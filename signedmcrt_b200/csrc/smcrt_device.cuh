@@ -246,23 +246,38 @@ template <> struct U01<double> {
     }
 };
 
-// Per-packet uniform stream: counter RNG keyed (seed, instance, packet id), or
-// an injected stream (replay mode).
+// One Philox block (out of line unless SMCRT_PHILOX_INLINE: one copy of the 10
+// rounds per kernel, at the cost of a call per four draws).
+#ifdef SMCRT_PHILOX_INLINE
+static __device__ __forceinline__ uint4 philox_block(
+#else
+static __device__ __noinline__ uint4 philox_block(
+#endif
+    uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t c2,
+                                                 uint32_t c3) {
+    uint32_t o[4];
+    philox4x32_10(k0, k1, c0, c1, c2, c3, o);
+    return make_uint4(o[0], o[1], o[2], o[3]);
+}
+
 // Per-packet uniform stream: counter RNG keyed (seed, instance, packet id); in
-// replay builds (INJ) an injected uniform stream instead.
+// replay builds (INJ) an injected uniform stream instead.  The key words live in
+// the caller's constant bank (seed, instance) and are passed at each refill.
 template <class R, bool INJ = false>
 struct Stream {
-    uint32_t k0, k1, inst, p0, p1, block;
+    uint32_t p0, p1, block;
     uint32_t b0, b1, b2, b3;  // unconsumed Philox words, consumed from b0 (register queue)
     int left;
     int ndraws;
     const double* inj;
     int ninj;
     int flags;
+    unsigned long long seed;
+    uint32_t inst;
 
-    __device__ __forceinline__ void init(uint64_t seed, uint32_t instance, uint64_t pid, const double* injected, int n) {
-        k0 = (uint32_t)seed;
-        k1 = (uint32_t)(seed >> 32);
+    __device__ __forceinline__ void init(uint64_t seed_, uint32_t instance, uint64_t pid, const double* injected,
+                                         int n) {
+        seed = seed_;
         inst = instance;
         p0 = (uint32_t)pid;
         p1 = (uint32_t)(pid >> 32);
@@ -283,12 +298,11 @@ struct Stream {
             return (R)inj[ndraws++];
         }
         if (left < U01<R>::kWords) {
-            uint32_t o[4];
-            philox4x32_10(k0, k1, block, inst, p0, p1, o);
-            b0 = o[0];
-            b1 = o[1];
-            b2 = o[2];
-            b3 = o[3];
+            const uint4 o = philox_block((uint32_t)seed, (uint32_t)(seed >> 32), block, inst, p0, p1);
+            b0 = o.x;
+            b1 = o.y;
+            b2 = o.z;
+            b3 = o.w;
             ++block;
             left = 4;
         }

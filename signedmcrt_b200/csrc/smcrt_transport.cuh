@@ -1,9 +1,13 @@
 // smcrt_transport.cuh -- the persistent, regenerating packet-transport kernel.
 //
-// One thread carries one packet at a time.  The loop body is ONE flight
-// (tauint2) per lane: a lane whose packet died launches a fresh packet at the
-// top of the next iteration (warp-aggregated work grab), so lanes do not idle
-// at the end of a long-lived packet the way a per-packet loop does.
+// One thread carries one packet at a time.  tauint2's nested loops (flights,
+// sphere-tracing steps, voxel walk) are flattened into a per-lane state
+// machine: every iteration of the persistent loop performs ONE short action --
+// launch a packet, sweep the SDFs, walk one voxel segment, handle a boundary,
+// interact, or retire a packet -- so lanes whose loops would run for different
+// trip counts stay busy instead of waiting at the end of the longest loop.
+// The arithmetic of each action is the same, operation for operation, as the
+// nested form in tauint2 (src/inttau2.f90:15-441).
 #pragma once
 
 #include "smcrt_device.cuh"
@@ -60,206 +64,6 @@ __device__ __forceinline__ V3<R> cv(V3<double> p) {
 template <class R>
 __device__ __forceinline__ V3<double> advance(V3<double> p, R d, V3<R> dir) {
     return V3<double>{p.x + (double)(d * dir.x), p.y + (double)(d * dir.y), p.z + (double)(d * dir.z)};
-}
-
-// Integer-stepping voxel walk over one sphere-tracing segment (the tally of
-// update_grids, src/inttau2.f90:213-292): same start cell (floor index,
-// :433-435) and grid-exit rule, with crossings advancing the index by +-1.
-template <class R>
-__device__ __forceinline__ void voxel_walk(const GridT<R>& g, double* __restrict__ jm, V3<R> pos, V3<R> dir, R L,
-                                           bool& tflag, Cnt& c) {
-    const V3<R> o{pos.x + g.xmax, pos.y + g.ymax, pos.z + g.zmax};
-    int ci = (int)floor((R)g.nx * o.x / ((R)2 * g.xmax)) + 1;
-    int cj = (int)floor((R)g.ny * o.y / ((R)2 * g.ymax)) + 1;
-    int ck = (int)floor((R)g.nz * o.z / ((R)2 * g.zmax)) + 1;
-    if (ci < 1 || ci > g.nx || cj < 1 || cj > g.ny || ck < 1 || ck > g.nz) {
-        tflag = true;
-        return;
-    }
-    const R big = (R)1e30;
-    const int sx = dir.x > (R)0 ? 1 : (dir.x < (R)0 ? -1 : 0);
-    const int sy = dir.y > (R)0 ? 1 : (dir.y < (R)0 ? -1 : 0);
-    const int sz = dir.z > (R)0 ? 1 : (dir.z < (R)0 ? -1 : 0);
-    R tx = big, ty = big, tz = big;
-    if (sx) tx = fmax(((R)(sx > 0 ? ci : ci - 1) * g.vx - o.x) / dir.x, (R)0);
-    if (sy) ty = fmax(((R)(sy > 0 ? cj : cj - 1) * g.vy - o.y) / dir.y, (R)0);
-    if (sz) tz = fmax(((R)(sz > 0 ? ck : ck - 1) * g.vz - o.z) / dir.z, (R)0);
-    long long idx = (long long)(ci - 1) + (long long)g.nx * ((long long)(cj - 1) + (long long)g.ny * (ck - 1));
-    const long long stride_y = g.nx, stride_z = (long long)g.nx * g.ny;
-    R d = 0;
-    for (;;) {
-        const R tm = fmin(tx, fmin(ty, tz));
-        if (tm > L) {
-            atomicAdd(jm + idx, (double)(L - d));
-            ++c.vox;
-            break;
-        }
-        atomicAdd(jm + idx, (double)(tm - d));
-        ++c.vox;
-        d = tm;
-        if (tm == tx) {
-            ci += sx;
-            if (ci < 1 || ci > g.nx) { tflag = true; break; }
-            idx += sx;
-            tx = fmax(((R)(sx > 0 ? ci : ci - 1) * g.vx - o.x) / dir.x, (R)0);
-        } else if (tm == ty) {
-            cj += sy;
-            if (cj < 1 || cj > g.ny) { tflag = true; break; }
-            idx += sy * stride_y;
-            ty = fmax(((R)(sy > 0 ? cj : cj - 1) * g.vy - o.y) / dir.y, (R)0);
-        } else {
-            ck += sz;
-            if (ck < 1 || ck > g.nz) { tflag = true; break; }
-            idx += sz * stride_z;
-            tz = fmax(((R)(sz > 0 ? ck : ck - 1) * g.vz - o.z) / dir.z, (R)0);
-        }
-    }
-}
-
-// tauint2, src/inttau2.f90:15-210
-template <class R, class Rng>
-__device__ __forceinline__ void tauint2(const Params<R>& P, double* __restrict__ jm, Pk<R>& pk, Rng& rng, Cnt& c) {
-    const SceneT<R>& sc = P.sc;
-    const int N = sc.nregions;
-    const R eps = P.eps;
-    const R inf = (R)INFINITY;
-    V3<double> pos = pk.pos, oldpos = pos;
-    V3<R> dir = pk.dir;
-    R tau = -log(rng.next());
-    R taurun = 0;
-    for (;;) {
-        R dsdf = inf;
-        {
-            const V3<R> pf = cv<R>(pos);
-            for (int i = 0; i < N; ++i) dsdf = fmin(dsdf, fabs(eval_region(sc, i, pf)));
-        }
-        c.sdf += N;
-        // The reference kills here when d < eps and stops tracing when d <= eps
-        // (inttau2.f90:58,63); a packet left at d == eps (reachable on the FP32
-        // coordinate grid) is treated as on the surface, like a reflected packet.
-        if (dsdf <= eps) {
-            pk.tflag = true;
-            break;
-        }
-        int steps = 0;
-        while (dsdf > eps) {
-            ++c.steps;
-            const R kap = sc.region[pk.layer].kappa;
-            const R tsdf = dsdf * kap;
-            bool last = false;
-            if (taurun + tsdf <= tau) {
-                taurun = taurun + tsdf;
-            } else {
-                dsdf = (tau - taurun) / kap;
-                taurun = tau;
-                last = true;
-            }
-            voxel_walk(P.grid, jm, cv<R>(pos), dir, dsdf, pk.tflag, c);
-            pos = advance(pos, dsdf, dir);
-            if (last) break;
-            R mn = inf, mna = inf;
-            const V3<R> pf = cv<R>(pos);
-            for (int i = 0; i < N; ++i) {
-                const R d = eval_region(sc, i, pf);
-                mn = fmin(mn, d);
-                mna = fmin(mna, fabs(d));
-            }
-            c.sdf += N;
-            dsdf = mna;
-            if (mn >= (R)0) {
-                pk.tflag = true;
-                break;
-            }
-            if (++steps >= P.max_steps) {
-                pk.tflag = true;
-                pk.flags |= STATUS_STEP_CAP;
-                break;
-            }
-        }
-        if (taurun >= tau || pk.tflag) break;
-
-        // Surface crossing (:104-184).  min|dstmp| equals the last sweep's dsdf
-        // (same position), so that sweep is counted but not repeated.
-        c.sdf += N;
-        const R dstep = dsdf + (R)2 * eps;
-        oldpos = pos;
-        pos = advance(pos, dstep, dir);
-        const int L = pk.layer;
-        int nl = -1;
-        R d0 = 0, dsL = 0, dsN = 0;
-        const V3<R> pf = cv<R>(pos);
-        for (int i = 0; i < N; ++i) {
-            const R d = eval_region(sc, i, pf);
-            if (i == 0) d0 = d;
-            if (i == L) dsL = d;
-            if (nl < 0 && d < (R)0) {
-                nl = i;
-                dsN = d;
-            }
-        }
-        c.sdf += N;
-        if (nl < 0) {
-            nl = 0;
-            dsN = d0;
-        }
-        const R n1 = sc.region[L].nidx, n2 = sc.region[nl].nidx;
-        if (n1 != n2) {
-            int which;
-            if (dsL < (R)0 && dsN < (R)0) {
-                which = (fabs(dsL) <= fabs(dsN)) ? L : nl;
-            } else {
-                const V3<R> of = cv<R>(oldpos);
-                const R tL = eval_region(sc, L, of), tN = eval_region(sc, nl, of);
-                if (tL < (R)0 && tN < (R)0) {
-                    which = (tL >= tN) ? L : nl;
-                } else if (dsL >= (R)0 && dsN < (R)0) {
-                    // An SDF value of exactly 0 counts as outside, like the `ds(i) < 0`
-                    // membership test; the reference's `error stop` branch (:155-156)
-                    // is then reached only by NaN.
-                    which = (L == 0) ? L : nl;  // oldlayer = packet%layer, then "== 1" test (:150-162)
-                } else if (dsL >= (R)0 && dsN >= (R)0) {
-                    pk.tflag = true;
-                    break;
-                } else {
-                    pk.tflag = true;  // "This should not be reached!" (:156)
-                    pk.flags |= STATUS_ERROR_STATE;
-                    break;
-                }
-            }
-            // Boundary event in FP64: calcNormal + reflect_refract (surfaces.f90:14-40).
-            ++c.fres;
-            c.sdf += 4;
-            const V3<double> Nn =
-                calc_normal(P.sc64, which, pos, P.normal_h);
-            V3<double> I{(double)dir.x, (double)dir.y, (double)dir.z};
-            const double m1 = P.sc64.region[L].nidx, m2 = P.sc64.region[nl].nidx;
-            const double Rf = fresnel(I, Nn, m1, m2);
-            const double u = (double)rng.next();
-            const bool refl = u <= Rf;
-            I = refl ? reflect(I, Nn) : refract(I, Nn, m1 / m2);
-            dir = V3<R>{(R)I.x, (R)I.y, (R)I.z};
-            pk.weight = pk.weight * (R)Rf;
-            tau = -log(rng.next());
-            taurun = 0;
-            if (!refl) {
-                pk.layer = nl;
-            } else {
-                ++c.refl;
-                pos = oldpos;
-                pk.bounces += 1;
-                if (pk.bounces > 1000) {
-                    pk.tflag = true;
-                    break;
-                }
-            }
-        } else {
-            pk.layer = nl;
-        }
-        if (pk.tflag) break;
-    }
-    pk.pos = pos;
-    pk.dir = dir;
-    if (fabs(pos.x) > P.grid.xmax_d || fabs(pos.y) > P.grid.ymax_d || fabs(pos.z) > P.grid.zmax_d) pk.tflag = true;
 }
 
 // Emitters, src/photon.f90
@@ -404,16 +208,17 @@ __device__ __forceinline__ long long detector_bin(const DetT& D, const double p[
     return D.off + idx - 1;
 }
 
+// Detector hits at packet death (kernelsMod.f90:302-306), out of line and by
+// value: it runs once per packet.
 template <class R>
-__device__ __forceinline__ void record_detectors(const Params<R>& P, const Buffers& B, const Pk<R>& pk) {
-    if (P.ndet == 0 || P.kernel == SMCRT_KERNEL_TEST) return;
-    const double p[3] = {(double)pk.pos.x, (double)pk.pos.y, (double)pk.pos.z};
-    const double l[3] = {(double)pk.dir.x, (double)pk.dir.y, (double)pk.dir.z};
-    const double value = (P.kernel == SMCRT_KERNEL_WEIGHT) ? (double)pk.weight
-                                                           : sqrt(pk.pos.x * pk.pos.x + pk.pos.y * pk.pos.y);
+__device__ __noinline__ void record_detectors(const Params<R>& P, double* bins, double px, double py, double pz,
+                                              double lx, double ly, double lz, double weight, int layer1) {
+    const double p[3] = {px, py, pz};
+    const double l[3] = {lx, ly, lz};
+    const double value = (P.kernel == SMCRT_KERNEL_WEIGHT) ? weight : sqrt(px * px + py * py);
     for (int d = 0; d < P.ndet; ++d) {
-        const long long b = detector_bin(P.det[d], p, l, value, pk.layer + 1);
-        if (b >= 0) atomicAdd(B.bins + b, 1.0);
+        const long long b = detector_bin(P.det[d], p, l, value, layer1);
+        if (b >= 0) atomicAdd(bins + b, 1.0);
     }
 }
 
@@ -426,106 +231,194 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // The persistent kernel.  KERNEL: smcrt_kernel_kind.  REPLAY: injected streams.
+#ifndef SMCRT_MIN_BLOCKS
+#define SMCRT_MIN_BLOCKS 3
+#endif
+#ifndef SMCRT_WALK_SEGMENTS
+#define SMCRT_WALK_SEGMENTS 4
+#endif
+
+// Per-lane actions of the flattened transport loop.
+enum Act : int { A_NEW = 0, A_SWEEP, A_WALK, A_CROSS, A_INTERACT, A_DEATH, A_DONE };
+// What the next sweep is for.
+enum SweepMode : int { S_LAUNCH = 0, S_TOP, S_STEP, S_CROSS };
+
+template <class R>
+struct Flight {
+    R tau, taurun, dsdf;  // optical depth to spend / spent; current step length
+    int steps;            // sphere-tracing steps of the current inner loop
+    int mode;             // SweepMode of the next sweep
+    bool last;            // the current step spends the remaining optical depth
+    // Integer voxel walk of the current step (update_grids, inttau2.f90:213-292):
+    // parametric distance to the next x/y/z face, distance walked, and the cell.
+    // During a crossing the same storage holds the position before the step.
+    union {
+        struct {
+            R tx, ty, tz, td;
+            int ci, cj, ck;
+        } w;
+        struct {
+            V3<double> oldpos;
+            int which, nl;
+        } x;
+    };
+};
+
+// One region at one point, out of line: used only on rare paths (crossings),
+// so the hot sweep stays the only inlined copy of the primitive switch.
+template <class R>
+__device__ __noinline__ R eval_region_cold(const SceneT<R>& sc, int r, V3<R> p) {
+    return eval_region(sc, r, p);
+}
+static __device__ __noinline__ V3<double> calc_normal_cold(const SceneT<double>& sc, int r, V3<double> p, double h) {
+    return calc_normal(sc, r, p, h);
+}
+
+// Step start in grid coordinates (the position does not move during a walk).
+template <class R>
+__device__ __forceinline__ V3<R> grid_origin(const GridT<R>& g, const V3<double>& pos) {
+    const V3<R> p = cv<R>(pos);
+    return V3<R>{p.x + g.xmax, p.y + g.ymax, p.z + g.zmax};
+}
+
+// Starts a sphere-tracing step of length f.dsdf (body of the while loop at
+// inttau2.f90:63-83): optical depth bookkeeping, then the voxel-walk setup.
+// Returns A_WALK, or -1 when the step starts outside the grid (no tally).
+template <class R>
+__device__ __forceinline__ int start_step(const Params<R>& P, const Pk<R>& pk, Flight<R>& f, Cnt& c, bool& tflag) {
+    ++c.steps;
+    const R kap = P.sc.region[pk.layer].kappa;
+    const R tsdf = f.dsdf * kap;
+    f.last = false;
+    if (f.taurun + tsdf <= f.tau) {
+        f.taurun = f.taurun + tsdf;
+    } else {
+        f.dsdf = (f.tau - f.taurun) / kap;
+        f.taurun = f.tau;
+        f.last = true;
+    }
+    const GridT<R>& g = P.grid;
+    const V3<R> o = grid_origin(g, pk.pos);
+    f.w.ci = (int)floor((R)g.nx * o.x / ((R)2 * g.xmax)) + 1;
+    f.w.cj = (int)floor((R)g.ny * o.y / ((R)2 * g.ymax)) + 1;
+    f.w.ck = (int)floor((R)g.nz * o.z / ((R)2 * g.zmax)) + 1;
+    if (f.w.ci < 1 || f.w.ci > g.nx || f.w.cj < 1 || f.w.cj > g.ny || f.w.ck < 1 || f.w.ck > g.nz) {
+        tflag = true;  // outside the grid: no tally for this step
+        return -1;
+    }
+    const R big = (R)1e30;
+    const V3<R>& d = pk.dir;
+    f.w.tx = d.x > (R)0 ? fmax(((R)f.w.ci * g.vx - o.x) / d.x, (R)0)
+           : d.x < (R)0 ? fmax(((R)(f.w.ci - 1) * g.vx - o.x) / d.x, (R)0) : big;
+    f.w.ty = d.y > (R)0 ? fmax(((R)f.w.cj * g.vy - o.y) / d.y, (R)0)
+           : d.y < (R)0 ? fmax(((R)(f.w.cj - 1) * g.vy - o.y) / d.y, (R)0) : big;
+    f.w.tz = d.z > (R)0 ? fmax(((R)f.w.ck * g.vz - o.z) / d.z, (R)0)
+           : d.z < (R)0 ? fmax(((R)(f.w.ck - 1) * g.vz - o.z) / d.z, (R)0) : big;
+    f.w.td = 0;
+    return A_WALK;
+}
+
+// One voxel segment of the current step; returns true when the step's walk is over.
+template <class R>
+__device__ __forceinline__ bool walk_segment(const GridT<R>& g, double* __restrict__ jm, const V3<double>& pos,
+                                             const V3<R>& d, Flight<R>& f, Cnt& c, bool& tflag) {
+    const R tm = fmin(f.w.tx, fmin(f.w.ty, f.w.tz));
+    const int idx = (f.w.ci - 1) + g.nx * ((f.w.cj - 1) + g.ny * (f.w.ck - 1));
+    ++c.vox;
+    if (tm > f.dsdf) {
+        atomicAdd(jm + idx, (double)(f.dsdf - f.w.td));
+        return true;
+    }
+    atomicAdd(jm + idx, (double)(tm - f.w.td));
+    f.w.td = tm;
+    const V3<R> o = grid_origin(g, pos);
+    if (tm == f.w.tx) {
+        const int s = d.x > (R)0 ? 1 : -1;
+        f.w.ci += s;
+        if (f.w.ci < 1 || f.w.ci > g.nx) { tflag = true; return true; }
+        f.w.tx = fmax(((R)(s > 0 ? f.w.ci : f.w.ci - 1) * g.vx - o.x) / d.x, (R)0);
+    } else if (tm == f.w.ty) {
+        const int s = d.y > (R)0 ? 1 : -1;
+        f.w.cj += s;
+        if (f.w.cj < 1 || f.w.cj > g.ny) { tflag = true; return true; }
+        f.w.ty = fmax(((R)(s > 0 ? f.w.cj : f.w.cj - 1) * g.vy - o.y) / d.y, (R)0);
+    } else {
+        const int s = d.z > (R)0 ? 1 : -1;
+        f.w.ck += s;
+        if (f.w.ck < 1 || f.w.ck > g.nz) { tflag = true; return true; }
+        f.w.tz = fmax(((R)(s > 0 ? f.w.ck : f.w.ck - 1) * g.vz - o.z) / d.z, (R)0);
+    }
+    return false;
+}
+
+// The end of a flight (inttau2.f90:188-209): grid-exit test, then interact or retire.
+template <class R>
+__device__ __forceinline__ int end_flight(const Params<R>& P, Pk<R>& pk) {
+    if (fabs(pk.pos.x) > P.grid.xmax_d || fabs(pk.pos.y) > P.grid.ymax_d || fabs(pk.pos.z) > P.grid.zmax_d)
+        pk.tflag = true;
+    return pk.tflag ? A_DEATH : A_INTERACT;
+}
+
+template <class R, class Rng>
+__device__ __forceinline__ void start_flight(Flight<R>& f, Rng& rng) {
+    f.tau = -log(rng.next());  // inttau2.f90:46
+    f.taurun = 0;
+}
+
+// Moves through a step that starts outside the grid (no walk), then continues.
+template <class R>
+__device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c) {
+    int a = start_step(P, pk, f, c, pk.tflag);
+    if (a < 0) {
+        pk.pos = advance(pk.pos, f.dsdf, pk.dir);
+        if (f.last) return end_flight(P, pk);
+        f.mode = S_STEP;
+        return A_SWEEP;
+    }
+    return a;
+}
+
+// The persistent kernel.  KERNEL: smcrt_kernel_kind.  REPLAY: injected streams.
+//
+// Each iteration runs the actions in a fixed order -- retire, launch,
+// interact, sweep, cross -- then walks voxel segments until no lane of the warp
+// has a segment left.  A lane can pass through several actions per iteration
+// (interact -> sweep -> walk), and lanes at different depths of their flights
+// stay in step because every phase is short.
 template <class R, int KERNEL, bool REPLAY>
-__global__ void __launch_bounds__(256, 2) transport_kernel(const __grid_constant__ Params<R> P, const Buffers B) {
+__global__ void __launch_bounds__(256, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
+                                                                          const Buffers B) {
     __shared__ unsigned long long s_cnt[C_NUM];
     __shared__ double s_mom[25];
     if (threadIdx.x < C_NUM) s_cnt[threadIdx.x] = 0ull;
     if (threadIdx.x < 25) s_mom[threadIdx.x] = 0.0;
     __syncthreads();
 
+    const SceneT<R>& sc = P.sc;
+    const int N = sc.nregions;
+    const R eps = P.eps;
     Pk<R> pk;
     pk.tflag = true;
+    pk.layer = 0;
+    Flight<R> f;
+    f.mode = S_LAUNCH;
     Stream<R, REPLAY> rng;
     Cnt c = {0, 0, 0, 0, 0, 0};
-    bool need_new = true;  // the lane holds no packet
+    int act = A_NEW;
     long long pid = 0;
     unsigned iter = 0;
     const unsigned long long t0 = P.budget_ns ? global_ns() : 0ull;
     for (;;) {
-        // device-side time budget: past it, stop between flights and flag ABORTED
-        if (P.budget_ns && ((++iter) & 63u) == 0u && global_ns() - t0 > P.budget_ns) {
+        // device-side time budget: past it, stop and flag ABORTED
+        if (P.budget_ns && ((++iter) & 255u) == 0u && global_ns() - t0 > P.budget_ns) {
             atomicOr(B.status, STATUS_ABORTED);
             break;
         }
-        // ---- prepare the next flight: a new packet (emit) or an interaction (scatter)
-        bool fly = true;
-        if (need_new) {
-            const unsigned m = __activemask();
-            const unsigned lane = lane_id();
-            const int leader = __ffs(m) - 1;
-            const unsigned rank = __popc(m & ((1u << lane) - 1u));
-            unsigned long long base = 0;
-            if ((int)lane == leader) base = atomicAdd(B.work, (unsigned long long)__popc(m));
-            base = __shfl_sync(m, base, leader);
-            pid = (long long)(base + rank);
-            if (pid >= P.count) break;
-            const long long gpid = P.first + pid;
-            if (REPLAY) {
-                const long long o0 = B.offsets[pid], o1 = B.offsets[pid + 1];
-                rng.init(P.seed, P.instance, (uint64_t)gpid, B.uniforms + o0, (int)(o1 - o0));
-            } else {
-                rng.init(P.seed, P.instance, (uint64_t)gpid, nullptr, 0);
-            }
-            emit(P, pk, rng);
-            pk.layer = launch_layer(P.sc, cv<R>(pk.pos));
-            c.sdf += P.sc.nregions;
-        } else if (KERNEL == SMCRT_KERNEL_WEIGHT) {  // weight_scatter, kernelsMod.f90:99-134
-            const DRegion<R>& rg = P.sc.region[pk.layer];
-            const R wa = pk.weight * ((R)1 - rg.albedo);
-            pk.weight = pk.weight - wa;
-            const R ox = (R)pk.pos.x + P.grid.xmax, oy = (R)pk.pos.y + P.grid.ymax, oz = (R)pk.pos.z + P.grid.zmax;
-            const int ci = (int)floor((R)P.grid.nx * ox / ((R)2 * P.grid.xmax)) + 1;
-            const int cj = (int)floor((R)P.grid.ny * oy / ((R)2 * P.grid.ymax)) + 1;
-            const int ck = (int)floor((R)P.grid.nz * oz / ((R)2 * P.grid.zmax)) + 1;
-            if (ci < 1 || ci > P.grid.nx || cj < 1 || cj > P.grid.ny || ck < 1 || ck > P.grid.nz) {
-                pk.tflag = true;
-                fly = false;
-            } else {
-                atomicAdd(B.jmean + (long long)(ci - 1) +
-                              (long long)P.grid.nx * ((long long)(cj - 1) + (long long)P.grid.ny * (ck - 1)),
-                          (double)wa);
-                pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
-                ++c.scat;
-                if (pk.weight < (R)0.01) {
-                    if (rng.next() < (R)0.1) pk.weight = pk.weight / (R)0.1;
-                    else {
-                        pk.tflag = true;
-                        fly = false;
-                    }
-                }
-            }
-        } else {  // pathlength_scatter :285-300 / test_kernel :408-436
-            const R ran = rng.next();
-            const DRegion<R>& rg = P.sc.region[pk.layer];
-            if (ran < rg.albedo) {
-                pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
-                ++c.scat;
-                pk.nscatt += 1;
-                if (KERNEL == SMCRT_KERNEL_TEST) {
-                    const int sidx = pk.nscatt;
-                    if (sidx >= 1 && sidx <= 4) {
-                        const double px = pk.pos.x, py = pk.pos.y, pz = pk.pos.z;
-                        atomicAdd(&s_mom[(sidx - 1) * 3 + 0], px);
-                        atomicAdd(&s_mom[(sidx - 1) * 3 + 1], py);
-                        atomicAdd(&s_mom[(sidx - 1) * 3 + 2], pz);
-                        atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 0], px * px);
-                        atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 1], py * py);
-                        atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 2], pz * pz);
-                    } else if (P.end_early) {
-                        pk.tflag = true;  // the reference still calls tauint2 once more (:428-435)
-                    }
-                }
-            } else {
-                pk.tflag = true;
-                fly = false;
-            }
-        }
-        // ---- one flight, from a single call site so the warp enters it together
-        if (fly) tauint2(P, B.jmean, pk, rng, c);
-        need_new = pk.tflag;
-        if (need_new) {
-            record_detectors(P, B, pk);
+        // ---- retire a finished packet: detectors (kernelsMod.f90:302-306), counters
+        if (act == A_DEATH) {
+            if (P.ndet > 0 && KERNEL != SMCRT_KERNEL_TEST)
+                record_detectors(P, B.bins, pk.pos.x, pk.pos.y, pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
+                                 (double)pk.dir.z, (double)pk.weight, pk.layer + 1);
             atomicAdd(&s_cnt[C_PACKETS], 1ull);
             atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);
             atomicAdd(&s_cnt[C_VOX], (unsigned long long)c.vox);
@@ -550,6 +443,237 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const __grid_constant
                 st.flags = fl;
             }
             c = Cnt{0, 0, 0, 0, 0, 0};
+            act = A_NEW;
+        }
+        // ---- take the next packet id (warp-aggregated) and emit it
+        if (act == A_NEW) {
+            const unsigned m = __activemask();
+            const unsigned lane = lane_id();
+            const int leader = __ffs(m) - 1;
+            const unsigned rank = __popc(m & ((1u << lane) - 1u));
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(B.work, (unsigned long long)__popc(m));
+            base = __shfl_sync(m, base, leader);
+            pid = (long long)(base + rank);
+            if (pid >= P.count) {
+                act = A_DONE;
+            } else {
+                const long long gpid = P.first + pid;
+                if (REPLAY) {
+                    const long long o0 = B.offsets[pid], o1 = B.offsets[pid + 1];
+                    rng.init(P.seed, P.instance, (uint64_t)gpid, B.uniforms + o0, (int)(o1 - o0));
+                } else {
+                    rng.init(P.seed, P.instance, (uint64_t)gpid, nullptr, 0);
+                }
+                emit(P, pk, rng);
+                start_flight(f, rng);
+                f.mode = S_LAUNCH;
+                act = A_SWEEP;
+            }
+        }
+        if (act == A_DONE) break;
+        // ---- between flights (kernelsMod.f90:285-300 / 99-134 / 408-436)
+        if (act == A_INTERACT) {
+            const DRegion<R>& rg = sc.region[pk.layer];
+            act = A_SWEEP;
+            if (KERNEL == SMCRT_KERNEL_WEIGHT) {
+                const R wa = pk.weight * ((R)1 - rg.albedo);
+                pk.weight = pk.weight - wa;
+                const R ox = (R)pk.pos.x + P.grid.xmax, oy = (R)pk.pos.y + P.grid.ymax, oz = (R)pk.pos.z + P.grid.zmax;
+                const int ci = (int)floor((R)P.grid.nx * ox / ((R)2 * P.grid.xmax)) + 1;
+                const int cj = (int)floor((R)P.grid.ny * oy / ((R)2 * P.grid.ymax)) + 1;
+                const int ck = (int)floor((R)P.grid.nz * oz / ((R)2 * P.grid.zmax)) + 1;
+                if (ci < 1 || ci > P.grid.nx || cj < 1 || cj > P.grid.ny || ck < 1 || ck > P.grid.nz) {
+                    pk.tflag = true;
+                    act = A_DEATH;
+                } else {
+                    atomicAdd(B.jmean + (ci - 1) + (long long)P.grid.nx * ((cj - 1) + (long long)P.grid.ny * (ck - 1)),
+                              (double)wa);
+                    pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
+                    ++c.scat;
+                    if (pk.weight < (R)0.01) {  // THRESHOLD, CHANCE (constants.f90:28-30)
+                        if (rng.next() < (R)0.1) pk.weight = pk.weight / (R)0.1;
+                        else {
+                            pk.tflag = true;
+                            act = A_DEATH;
+                        }
+                    }
+                }
+            } else {
+                const R ran = rng.next();
+                if (ran < rg.albedo) {
+                    pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
+                    ++c.scat;
+                    pk.nscatt += 1;
+                    if (KERNEL == SMCRT_KERNEL_TEST) {
+                        const int sidx = pk.nscatt;
+                        if (sidx >= 1 && sidx <= 4) {
+                            const double px = pk.pos.x, py = pk.pos.y, pz = pk.pos.z;
+                            atomicAdd(&s_mom[(sidx - 1) * 3 + 0], px);
+                            atomicAdd(&s_mom[(sidx - 1) * 3 + 1], py);
+                            atomicAdd(&s_mom[(sidx - 1) * 3 + 2], pz);
+                            atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 0], px * px);
+                            atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 1], py * py);
+                            atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 2], pz * pz);
+                        } else if (P.end_early) {
+                            pk.tflag = true;  // the reference still calls tauint2 once more (:428-435)
+                        }
+                    }
+                } else {
+                    pk.tflag = true;
+                    act = A_DEATH;
+                }
+            }
+            if (act == A_SWEEP) {
+                start_flight(f, rng);
+                f.mode = S_TOP;
+            }
+        }
+        // ---- evaluate every region at the current position (the one inlined sweep)
+        if (act == A_SWEEP) {
+            const V3<R> pf = cv<R>(pk.pos);
+            const int L = pk.layer;
+            R mn = (R)INFINITY, mna = (R)INFINITY, inner = (R)INFINITY;
+            R d0 = 0, dsL = 0, dsN = 0;
+            int nl = -1, lay = 0;
+            for (int i = 0; i < N; ++i) {
+                const R d = eval_region(sc, i, pf);
+                mn = fmin(mn, d);
+                mna = fmin(mna, fabs(d));
+                if (i == 0) d0 = d;
+                if (i == L) dsL = d;
+                if (nl < 0 && d < (R)0) {
+                    nl = i;
+                    dsN = d;
+                }
+                // launch layer (kernelsMod.f90:275-280): innermost containing region
+                const R a = (d > (R)0) ? (R)999.0 : fabs(d);
+                if (a < inner) {
+                    inner = a;
+                    lay = i;
+                }
+            }
+            c.sdf += N;
+            f.dsdf = mna;
+            const int mode = f.mode;
+            if (mode == S_LAUNCH || mode == S_TOP) {
+                // top of tauint2's outer loop (:51-61).  At launch the same sweep also
+                // gives the layer (the reference evaluates the same point twice).
+                if (mode == S_LAUNCH) {
+                    pk.layer = lay;
+                    c.sdf += N;
+                }
+                f.steps = 0;
+                // d == eps (reachable on the FP32 coordinate grid) counts as on the
+                // surface, like the reflected packets the reference kills here
+                if (mna <= eps) {
+                    pk.tflag = true;
+                    act = end_flight(P, pk);
+                } else {
+                    act = step_or_skip(P, pk, f, c);
+                }
+            } else if (mode == S_STEP) {
+                if (mn >= (R)0) {  // outside every region (:92-96)
+                    pk.tflag = true;
+                    act = end_flight(P, pk);
+                } else if (++f.steps >= P.max_steps) {
+                    pk.tflag = true;
+                    pk.flags |= STATUS_STEP_CAP;
+                    act = end_flight(P, pk);
+                } else if (mna > eps) {
+                    act = step_or_skip(P, pk, f, c);
+                } else if (f.taurun >= f.tau || pk.tflag) {
+                    act = end_flight(P, pk);  // (:99-102)
+                } else {
+                    // surface reached: count the reference's dstmp sweep (values of this
+                    // one, :104-108) and take the crossing step of min|d| + 2 eps
+                    c.sdf += N;
+                    f.x.oldpos = pk.pos;
+                    pk.pos = advance(pk.pos, mna + (R)2 * eps, pk.dir);
+                    f.mode = S_CROSS;
+                    act = A_SWEEP + 100;  // sweep again at the new position (next iteration)
+                }
+            } else {  // S_CROSS: sweep at the stepped position (:117-184)
+                if (nl < 0) {
+                    nl = 0;
+                    dsN = d0;
+                }
+                act = A_CROSS;
+                f.mode = S_TOP;
+                if (sc.region[L].nidx != sc.region[nl].nidx) {
+                    int which = -1;
+                    if (dsL < (R)0 && dsN < (R)0) {
+                        which = (fabs(dsL) <= fabs(dsN)) ? L : nl;
+                    } else {
+                        const V3<R> of = cv<R>(f.x.oldpos);
+                        const R tL = eval_region_cold(sc, L, of), tN = eval_region_cold(sc, nl, of);
+                        if (tL < (R)0 && tN < (R)0) {
+                            which = (tL >= tN) ? L : nl;
+                        } else if (dsL >= (R)0 && dsN < (R)0) {
+                            // exactly 0 counts as outside, like the `ds(i) < 0` membership
+                            // test; the `error stop` branch (:155-156) is then reached only by NaN
+                            which = (L == 0) ? L : nl;  // oldlayer = packet%layer, then "== 1" (:150-162)
+                        } else if (dsL >= (R)0 && dsN >= (R)0) {
+                            pk.tflag = true;
+                        } else {
+                            pk.tflag = true;
+                            pk.flags |= STATUS_ERROR_STATE;
+                        }
+                    }
+                    f.x.which = which;  // the boundary event runs in the A_CROSS phase below
+                    f.x.nl = nl;
+                } else {
+                    pk.layer = nl;
+                    f.x.which = -2;  // same refractive index: continue with the same tau
+                }
+                if (pk.tflag) act = end_flight(P, pk);
+            }
+        }
+        if (act == A_SWEEP + 100) act = A_SWEEP;
+        // ---- boundary event in FP64: calcNormal + reflect_refract (surfaces.f90:14-40)
+        if (act == A_CROSS) {
+            act = A_SWEEP;
+            const int which = f.x.which;
+            if (which >= 0) {
+                const int L = pk.layer, nl = f.x.nl;
+                ++c.fres;
+                c.sdf += 4;
+                const V3<double> Nn = calc_normal_cold(P.sc64, which, pk.pos, P.normal_h);
+                V3<double> I{(double)pk.dir.x, (double)pk.dir.y, (double)pk.dir.z};
+                const double m1 = P.sc64.region[L].nidx, m2 = P.sc64.region[nl].nidx;
+                const double Rf = fresnel(I, Nn, m1, m2);
+                const double u = (double)rng.next();
+                const bool refl = u <= Rf;
+                I = refl ? reflect(I, Nn) : refract(I, Nn, m1 / m2);
+                pk.dir = V3<R>{(R)I.x, (R)I.y, (R)I.z};
+                pk.weight = pk.weight * (R)Rf;
+                f.tau = -log(rng.next());
+                f.taurun = 0;
+                if (!refl) {
+                    pk.layer = nl;
+                } else {
+                    ++c.refl;
+                    pk.pos = f.x.oldpos;
+                    pk.bounces += 1;
+                    if (pk.bounces > 1000) {
+                        pk.tflag = true;
+                        act = end_flight(P, pk);
+                    }
+                }
+            }
+        }
+        // ---- walk voxel segments: at most SMCRT_WALK_SEGMENTS per lane per
+        // iteration, so one long walk does not hold up the other lanes' actions
+        for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
+            if (walk_segment(P.grid, B.jmean, pk.pos, pk.dir, f, c, pk.tflag)) {
+                pk.pos = advance(pk.pos, f.dsdf, pk.dir);
+                if (f.last) {
+                    act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
+                } else {
+                    f.mode = S_STEP;
+                    act = A_SWEEP;
+                }
+            }
         }
     }
     __syncthreads();

@@ -53,7 +53,9 @@ class Transport:
         o.eps, o.normal_h = eps, normal_h
         o.instance = instance
         o.timeout_ms = timeout_ms
-        o.stream = stream
+        # stream=None: a stream private to this context; an int: that cudaStream_t (0 = default)
+        o.stream = stream if stream is not None else None
+        o.private_stream = int(stream is None)
         self.options = o
         self.kernel, self.precision = kernel, precision
         self._ctx = C.c_void_p()
