@@ -257,6 +257,27 @@ int32_t smcrt_run_batched(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* 
                           const uint64_t* seeds, double* const* jmeans,
                           double* const* det_bins, smcrt_stats* stats);
 
+/* Allocation-free form of smcrt_run_device, for callers that cannot allocate
+ * device memory (inside a CUDA stream capture, under an application-owned memory
+ * pool, or with device memory budgeted up front).  It takes the same inputs as
+ * smcrt_create plus caller-owned DEVICE tally buffers, creates no context, and
+ * calls no cudaMalloc/cudaFree: the kernel's scratch (work counter, event
+ * counters, status) is a static device array of smcrt_static_scratch_bytes()
+ * bytes inside the library, present on every GPU that loads it until exit.
+ * ADDS the tallies of packets [first, first+count) into jmean_dev/det_bins_dev
+ * on opts->stream (NULL = default stream).  The first call on a device resolves
+ * the array's device address; make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU race on it.
+ * If stats is not NULL the call synchronises the stream and fills it.
+ * No counterpart in the reference (signedMCRT allocates its tallies itself). */
+int32_t smcrt_run_device_static(const smcrt_scene* scene, const smcrt_grid* grid,
+                                const smcrt_source* source, const smcrt_detector* dets,
+                                int32_t ndet, const smcrt_options* opts, int64_t first,
+                                int64_t count, uint64_t seed, double* jmean_dev,
+                                double* det_bins_dev, smcrt_stats* stats);
+/* Size of the static scratch array used by smcrt_run_device_static. */
+int64_t smcrt_static_scratch_bytes(void);
+
 /* ---- device-function probes (parity of the building blocks) --------------- */
 /* Evaluates every region's SDF at npts points (xyz triples); out[p*nregions+r]. */
 int32_t smcrt_eval_sdf(const smcrt_scene* scene, int32_t precision,

@@ -136,6 +136,10 @@ SIGNATURES = {
     "smcrt_run_batched": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_uint64),
                            C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_double)), C.POINTER(Stats)],
                           C.c_int32),
+    "smcrt_run_device_static": ([C.POINTER(Scene), C.POINTER(Grid), C.POINTER(Source), C.POINTER(Detector),
+                                 C.c_int32, C.POINTER(Options), C.c_int64, C.c_int64, C.c_uint64, C.c_void_p,
+                                 C.c_void_p, C.POINTER(Stats)], C.c_int32),
+    "smcrt_static_scratch_bytes": ([], C.c_int64),
     "smcrt_eval_sdf": ([C.POINTER(Scene), C.c_int32, C.POINTER(C.c_double), C.c_int64, C.POINTER(C.c_double)],
                        C.c_int32),
     "smcrt_calc_normal": ([C.POINTER(Scene), C.c_int32, C.c_double, C.POINTER(C.c_double), C.c_int64,

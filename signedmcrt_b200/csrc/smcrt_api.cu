@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -234,9 +235,8 @@ int occupancy_grid(smcrt_ctx* c, int precision, int kernel, int blocks_per_sm) {
 }
 
 template <class R>
-Params<R>* make_params(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* src,
-                       const DetT* dets, int ndet, const smcrt_options* o) {
-    Params<R>* P = new Params<R>;
+void fill_params(Params<R>* P, const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* src,
+                 const DetT* dets, int ndet, const smcrt_options* o) {
     std::memset(P, 0, sizeof(*P));
     fill_scene(P->sc, scene);
     fill_scene(P->sc64, scene);
@@ -252,6 +252,13 @@ Params<R>* make_params(const smcrt_scene* scene, const smcrt_grid* grid, const s
     P->normal_h = (o && o->normal_h > 0) ? o->normal_h : 1e-6;
     P->instance = o ? o->instance : 0u;
     P->budget_ns = (unsigned long long)((o && o->timeout_ms > 0) ? o->timeout_ms : 600000) * 1000000ull;
+}
+
+template <class R>
+Params<R>* make_params(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* src,
+                       const DetT* dets, int ndet, const smcrt_options* o) {
+    Params<R>* P = new Params<R>;
+    fill_params(P, scene, grid, src, dets, ndet, o);
     return P;
 }
 
@@ -547,6 +554,178 @@ int32_t smcrt_run_batched(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* 
                           double* const* jmeans, double* const* det_bins, smcrt_stats* stats) {
     g_err.clear();
     return fail(SMCRT_ERR_ARG, "smcrt_run_batched: not available in this build");
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free run.  Some callers cannot allocate device memory at all: code
+// running inside a CUDA stream capture, host applications that own every byte of
+// device memory through their own pool, or processes whose memory is reserved up
+// front for a fixed budget.  smcrt_run_device_static serves them: it creates no
+// context and calls no cudaMalloc/cudaFree.  The transport kernel's scratch (the
+// packet-work counter, the event counters, the device status word) lives in the
+// file-scope array below, loaded with the library on every GPU that uses it and
+// held until the process exits.  Every call shares this one array, so calls that
+// overlap on the GPU (different streams or threads) race on it.
+}  // extern "C"
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = 4096;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Scratch layout: [work u64][C_NUM counters u64][25 moments f64][status i32].
+constexpr size_t kScratchCounters = sizeof(unsigned long long) * (1 + C_NUM);
+constexpr size_t kScratchMoments = sizeof(double) * 25;
+constexpr size_t kScratchNeeded = kScratchCounters + kScratchMoments + sizeof(int);
+
+constexpr int kMaxDevices = 64;
+unsigned char* g_scratch_dev[kMaxDevices] = {};
+std::mutex g_scratch_mu;
+
+// Device address of the static scratch on the current device, resolved once per
+// device (the host-side name g_static_scratch is not a device address).
+int static_scratch(int dev, unsigned char** out) {
+    if (dev < 0 || dev >= kMaxDevices) return fail(SMCRT_ERR_ARG, "static run: device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_dev[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(SMCRT_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+        g_scratch_dev[dev] = (unsigned char*)p;
+    }
+    *out = g_scratch_dev[dev];
+    return SMCRT_OK;
+}
+
+template <class R>
+int run_static_t(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* source,
+                 const smcrt_detector* dets, int32_t ndet, const smcrt_options* opts, long long first,
+                 long long count, uint64_t seed, double* jmean_dev, double* bins_dev, smcrt_stats* stats) {
+    DetT dtab[kMaxDetectors];
+    long long nbins = 0;
+    int rc = fill_dets(dtab, dets, ndet, scene->nregions, nbins);
+    if (rc) return rc;
+    if (nbins > 0 && !bins_dev) return fail(SMCRT_ERR_ARG, "static run: detector bins buffer is null");
+    int dev = 0, nsm = 0;
+    rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    unsigned char* scratch = nullptr;
+    rc = static_scratch(dev, &scratch);
+    if (rc) return rc;
+    const int kern = opts ? opts->kernel : SMCRT_KERNEL_PATHLENGTH;
+    const int block = (opts && opts->block_size > 0) ? opts->block_size : 256;
+    if (block > 256 || block % 32) return fail(SMCRT_ERR_ARG, "options: block_size must be a multiple of 32 <= 256");
+    // the launch parameters live on this host stack (no heap, no device memory)
+    Params<R> P;
+    fill_params(&P, scene, grid, source, dtab, ndet, opts);
+    P.first = first;
+    P.count = count;
+    P.seed = seed;
+    int per_sm = 0;
+    cudaError_t e;
+    if constexpr (sizeof(R) == 8)
+        e = kern == SMCRT_KERNEL_WEIGHT ? occupancy_f64_1(block, &per_sm)
+          : kern == SMCRT_KERNEL_TEST   ? occupancy_f64_2(block, &per_sm) : occupancy_f64_0(block, &per_sm);
+    else
+        e = kern == SMCRT_KERNEL_WEIGHT ? occupancy_f32_1(block, &per_sm)
+          : kern == SMCRT_KERNEL_TEST   ? occupancy_f32_2(block, &per_sm) : occupancy_f32_0(block, &per_sm);
+    if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
+    if (per_sm < 1) per_sm = 1;
+    if (opts && opts->blocks_per_sm > 0 && opts->blocks_per_sm < per_sm) per_sm = opts->blocks_per_sm;
+    const long long need = (count + block - 1) / block;
+    const int blocks = (int)std::min<long long>((long long)nsm * per_sm, std::max<long long>(need, 1));
+    cudaStream_t s = opts ? (cudaStream_t)opts->stream : (cudaStream_t)0;
+    // the scratch keeps the previous call's values: clear what must start at zero
+    CK(cudaMemsetAsync(scratch, 0, kScratchNeeded, s));
+    Buffers B;
+    B.jmean = jmean_dev;
+    B.bins = bins_dev;
+    B.work = (unsigned long long*)scratch;
+    B.counters = (unsigned long long*)scratch + 1;
+    B.moments = (double*)(scratch + kScratchCounters);
+    B.status = (int*)(scratch + kScratchCounters + kScratchMoments);
+    B.uniforms = nullptr;
+    B.offsets = nullptr;
+    B.states = nullptr;
+    if constexpr (sizeof(R) == 8)
+        e = kern == SMCRT_KERNEL_WEIGHT ? launch_f64_1(P, B, false, blocks, block, s)
+          : kern == SMCRT_KERNEL_TEST   ? launch_f64_2(P, B, false, blocks, block, s)
+                                        : launch_f64_0(P, B, false, blocks, block, s);
+    else
+        e = kern == SMCRT_KERNEL_WEIGHT ? launch_f32_1(P, B, false, blocks, block, s)
+          : kern == SMCRT_KERNEL_TEST   ? launch_f32_2(P, B, false, blocks, block, s)
+                                        : launch_f32_0(P, B, false, blocks, block, s);
+    if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    if (!stats) return SMCRT_OK;
+    CK(cudaStreamSynchronize(s));
+    unsigned long long cnt[1 + C_NUM];
+    double mom[25];
+    int status = 0;
+    CK(cudaMemcpy(cnt, scratch, sizeof(cnt), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(mom, scratch + kScratchCounters, sizeof(mom), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&status, scratch + kScratchCounters + kScratchMoments, sizeof(int), cudaMemcpyDeviceToHost));
+    std::memset(stats, 0, sizeof(*stats));
+    const unsigned long long* k = cnt + 1;
+    stats->packets = k[C_PACKETS];
+    stats->sdf_evals = k[C_SDF];
+    stats->voxel_segments = k[C_VOX];
+    stats->trace_steps = k[C_STEPS];
+    stats->scatters = k[C_SCAT];
+    stats->fresnel_events = k[C_FRES];
+    stats->reflections = k[C_REFL];
+    stats->kills_step_cap = k[C_STEPCAP];
+    stats->kills_error = k[C_ERR];
+    stats->rng_draws = k[C_DRAWS];
+    for (int i = 0; i < 24; ++i) stats->moments[i] = mom[i];
+    stats->nscatt = mom[24];
+    stats->device_status = status;
+    if (status & STATUS_ABORTED) return fail(SMCRT_ERR_TIMEOUT, "transport kernel reached its time limit and stopped early");
+    return SMCRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t smcrt_static_scratch_bytes(void) { return (int64_t)kStaticScratchBytes; }
+
+int32_t smcrt_run_device_static(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* source,
+                                const smcrt_detector* dets, int32_t ndet, const smcrt_options* opts, int64_t first,
+                                int64_t count, uint64_t seed, double* jmean_dev, double* det_bins_dev,
+                                smcrt_stats* stats) {
+    g_err.clear();
+    // one run needs the work counter, the event counters, the moments and the
+    // status word; the array is sized for that and a larger need is refused
+    if (kScratchNeeded > kStaticScratchBytes)
+        return fail(SMCRT_ERR_ARG, "static run: the kernel needs " + std::to_string(kScratchNeeded) +
+                                       " bytes of scratch, the library's static array holds " +
+                                       std::to_string(kStaticScratchBytes));
+    int rc = validate_scene(scene);
+    if (rc) return rc;
+    rc = validate_optics(scene);
+    if (rc) return rc;
+    if (!grid || grid->nxg <= 0 || grid->nyg <= 0 || grid->nzg <= 0 || !(grid->xmax > 0) || !(grid->ymax > 0) ||
+        !(grid->zmax > 0))
+        return fail(SMCRT_ERR_ARG, "grid: need positive voxel counts and half sizes");
+    if ((long long)grid->nxg * grid->nyg * grid->nzg > (1ll << 31))
+        return fail(SMCRT_ERR_ARG, "grid: more than 2^31 voxels");
+    if (!source || source->kind < SMCRT_SRC_POINT || source->kind > SMCRT_SRC_FOCUS)
+        return fail(SMCRT_ERR_ARG, "source: unknown kind");
+    if (ndet < 0 || ndet > kMaxDetectors || (ndet > 0 && !dets))
+        return fail(SMCRT_ERR_ARG, "detectors: 0.." + std::to_string(kMaxDetectors) + " supported");
+    if (!jmean_dev) return fail(SMCRT_ERR_ARG, "static run: fluence buffer is null");
+    if (first < 0 || count < 0) return fail(SMCRT_ERR_ARG, "negative packet range");
+    if (opts && opts->kernel != SMCRT_KERNEL_PATHLENGTH && opts->kernel != SMCRT_KERNEL_WEIGHT &&
+        opts->kernel != SMCRT_KERNEL_TEST)
+        return fail(SMCRT_ERR_ARG, "options: unknown kernel");
+    const int prec = opts ? opts->precision : SMCRT_FP32;
+    if (prec == SMCRT_FP64)
+        return run_static_t<double>(scene, grid, source, dets, ndet, opts, first, count, seed, jmean_dev, det_bins_dev,
+                                    stats);
+    if (prec != SMCRT_FP32) return fail(SMCRT_ERR_ARG, "options: unknown precision");
+    return run_static_t<float>(scene, grid, source, dets, ndet, opts, first, count, seed, jmean_dev, det_bins_dev,
+                               stats);
 }
 
 int32_t smcrt_eval_sdf(const smcrt_scene* scene, int32_t precision, const double* pts, int64_t npts, double* out) {
