@@ -174,7 +174,12 @@ typedef struct smcrt_options {
     void* stream;          /* cudaStream_t to launch on; NULL = the default stream */
     int32_t private_stream;/* nonzero: the context creates and owns a non-blocking stream
                               and ignores `stream` */
-    int32_t reserved2;
+    int32_t tally_copies;  /* copies of the fluence grid that the CTAs spread their
+                              atomic adds over, summed after the launch (no
+                              counterpart in the reference; the sum is the same
+                              tally): 0 = library choice (as many as fit in
+                              64 MiB, at most 8), 1 = a single grid, up to 16;
+                              rounded down to a power of two */
 } smcrt_options;
 
 /* Event counters of one run (definitions identical in the CPU oracle). */

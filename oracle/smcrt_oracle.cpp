@@ -517,18 +517,19 @@ bool update_grids_int(const GridD& g, V3<R> pos, V3<R> dir, R dsdf, Tally& t, Co
         t.add(cell_index(g, ci, cj, ck), (double)(tm - d));
         ++c.vox;
         d = tm;
+        // next face on the crossed axis: one face spacing v/|d| further (Amanatides & Woo)
         if (tm == tx) {
             ci += sx;
             if (ci < 1 || ci > g.nx) { tflag = true; break; }
-            tx = tnext(ci, sx, vx, o.x, dir.x);
+            tx = tm + vx / std::fabs(dir.x);
         } else if (tm == ty) {
             cj += sy;
             if (cj < 1 || cj > g.ny) { tflag = true; break; }
-            ty = tnext(cj, sy, vy, o.y, dir.y);
+            ty = tm + vy / std::fabs(dir.y);
         } else {
             ck += sz;
             if (ck < 1 || ck > g.nz) { tflag = true; break; }
-            tz = tnext(ck, sz, vz, o.z, dir.z);
+            tz = tm + vz / std::fabs(dir.z);
         }
     }
     return true;

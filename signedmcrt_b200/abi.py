@@ -67,7 +67,7 @@ class Options(C.Structure):
                 ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("max_trace_steps", C.c_int32),
                 ("eps", C.c_double), ("normal_h", C.c_double), ("instance", C.c_uint32),
                 ("timeout_ms", C.c_int32), ("stream", C.c_void_p), ("private_stream", C.c_int32),
-                ("reserved2", C.c_int32)]
+                ("tally_copies", C.c_int32)]
 
 
 class Stats(C.Structure):

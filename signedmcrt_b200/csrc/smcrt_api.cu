@@ -192,7 +192,31 @@ int pick_device(int& dev, int& nsm) {
     return SMCRT_OK;
 }
 
+// Sums the fluence-grid copies into the output grid and zeroes them for the
+// next launch: cells are independent, one coalesced grid-stride pass.
+__global__ void __launch_bounds__(256) reduce_copies_kernel(double* __restrict__ out, double* __restrict__ copies,
+                                                            int ncopies, long long ncell) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ncell; i += stride) {
+        double sum = 0.0;
+        for (int k = 0; k < ncopies; ++k) {
+            double* q = copies + (long long)k * ncell + i;
+            sum += *q;
+            *q = 0.0;
+        }
+        if (sum != 0.0) out[i] += sum;
+    }
+}
+
 }  // namespace
+
+cudaError_t smcrt::reduce_tally_copies(double* out, double* copies, int ncopies, long long ncell, int nsm,
+                                       cudaStream_t s) {
+    const long long need = (ncell + 255) / 256;
+    const int blocks = (int)std::min<long long>(need, (long long)nsm * 8);
+    reduce_copies_kernel<<<blocks, 256, 0, s>>>(out, copies, ncopies, ncell);
+    return cudaGetLastError();
+}
 
 // ===========================================================================
 struct smcrt_ctx {
@@ -203,7 +227,9 @@ struct smcrt_ctx {
     Params<float>* pf = nullptr;
     Params<double>* pd = nullptr;
     long long ncell = 0, nbins = 0;
+    int tcopies = 1;                          // fluence-grid copies (1 = the output grid only)
     double* d_jmean = nullptr;
+    double* d_copies = nullptr;               // tcopies - 1 zeroed copies
     double* d_bins = nullptr;
     unsigned long long* d_work = nullptr;     // [0] work, [1..C_NUM] counters
     double* d_mom = nullptr;                  // 25
@@ -215,22 +241,55 @@ struct smcrt_ctx {
 
 namespace {
 
-int occupancy_grid(smcrt_ctx* c, int precision, int kernel, int blocks_per_sm) {
+// Detector bins counted per CTA in shared memory: all of them when they fit,
+// else none.  A CTA's count of one bin is at most the packets of the launch, so
+// launches of 2^32 packets or more use the global bins.
+int shared_bins(long long nbins, long long count) {
+    return (nbins > 0 && nbins <= kMaxSharedBins && count < (1ll << 32)) ? (int)nbins : 0;
+}
+
+// Resident CTAs per SM of the transport kernel with `smem` bytes of dynamic
+// shared memory, capped by the caller's blocks_per_sm.
+int resident_per_sm(int precision, int kernel, int block, size_t smem, int blocks_per_sm, int* out) {
     int per_sm = 0;
     cudaError_t e;
     if (precision == SMCRT_FP64) {
-        e = kernel == SMCRT_KERNEL_WEIGHT ? occupancy_f64_1(c->block, &per_sm)
-            : kernel == SMCRT_KERNEL_TEST ? occupancy_f64_2(c->block, &per_sm)
-                                          : occupancy_f64_0(c->block, &per_sm);
+        e = kernel == SMCRT_KERNEL_WEIGHT ? occupancy_f64_1(block, smem, &per_sm)
+            : kernel == SMCRT_KERNEL_TEST ? occupancy_f64_2(block, smem, &per_sm)
+                                          : occupancy_f64_0(block, smem, &per_sm);
     } else {
-        e = kernel == SMCRT_KERNEL_WEIGHT ? occupancy_f32_1(c->block, &per_sm)
-            : kernel == SMCRT_KERNEL_TEST ? occupancy_f32_2(c->block, &per_sm)
-                                          : occupancy_f32_0(c->block, &per_sm);
+        e = kernel == SMCRT_KERNEL_WEIGHT ? occupancy_f32_1(block, smem, &per_sm)
+            : kernel == SMCRT_KERNEL_TEST ? occupancy_f32_2(block, smem, &per_sm)
+                                          : occupancy_f32_0(block, smem, &per_sm);
     }
     if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
     if (per_sm < 1) per_sm = 1;
     if (blocks_per_sm > 0 && blocks_per_sm < per_sm) per_sm = blocks_per_sm;
+    *out = per_sm;
+    return SMCRT_OK;
+}
+
+int occupancy_grid(smcrt_ctx* c, int precision, int kernel, int blocks_per_sm) {
+    int per_sm = 0;
+    const size_t smem = sizeof(unsigned) * (size_t)shared_bins(c->nbins, 0);
+    int rc = resident_per_sm(precision, kernel, c->block, smem, blocks_per_sm, &per_sm);
+    if (rc) return rc;
     c->grid_blocks = c->nsm * per_sm;
+    return SMCRT_OK;
+}
+
+// Fluence-grid copies: the requested number, or as many as fit in 64 MiB (at
+// most 8), rounded down to a power of two.  Copies spread the atomic adds of
+// packets that share voxels (a pencil beam's axis) over several addresses.
+int tally_copies(const smcrt_options* o, long long ncell, int* out) {
+    const int req = o ? o->tally_copies : 0;
+    if (req < 0 || req > kMaxTallyCopies)
+        return fail(SMCRT_ERR_ARG, "options: tally_copies must be 0.." + std::to_string(kMaxTallyCopies));
+    const long long budget = 64ll << 20;
+    const long long want = req > 0 ? req : std::max(1ll, std::min(8ll, budget / (8ll * ncell)));
+    int tc = 1;  // rounded down to a power of two (the kernel picks a copy by a mask)
+    while (tc * 2 <= want) tc *= 2;
+    *out = tc;
     return SMCRT_OK;
 }
 
@@ -251,6 +310,9 @@ void fill_params(Params<R>* P, const smcrt_scene* scene, const smcrt_grid* grid,
     P->eps = (R)((o && o->eps > 0) ? o->eps : default_eps(prec, *grid));
     P->normal_h = (o && o->normal_h > 0) ? o->normal_h : 1e-6;
     P->instance = o ? o->instance : 0u;
+    P->tcopies = 1;
+    P->tmask = 0;
+    P->ncell = (long long)grid->nxg * grid->nyg * grid->nzg;
     P->budget_ns = (unsigned long long)((o && o->timeout_ms > 0) ? o->timeout_ms : 600000) * 1000000ull;
 }
 
@@ -291,6 +353,14 @@ int launch_f64(smcrt_ctx* c, const Params<double>& P, const Buffers& B, bool rep
     return SMCRT_OK;
 }
 
+template <class R>
+void set_tally_table(Params<R>* P, double* jm, double* copies, int tc, long long ncell) {
+    P->tcopies = tc;
+    P->tmask = (unsigned)(tc - 1);
+    for (int k = 0; k < kMaxTallyCopies; ++k)
+        P->jtab[k] = (k == 0) ? jm : (k < tc ? copies + (long long)(k - 1) * ncell : nullptr);
+}
+
 // Enqueues: reset work/counters/status, then the kernel for [first, first+count).
 int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, double* jm, double* bins, bool replay,
             const double* d_u, const long long* d_off, smcrt_packet_state* d_states) {
@@ -303,16 +373,28 @@ int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, doubl
     B.states = d_states;
     long long need = (count + c->block - 1) / c->block;
     int blocks = (int)std::min<long long>(c->grid_blocks, std::max<long long>(need, 1));
+    const int sb = shared_bins(c->nbins, count);
+    int tc = 1;  // a power of two, at most one copy per CTA
+    while (tc * 2 <= std::min(c->tcopies, blocks)) tc *= 2;
+    int rc;
     if (c->precision == SMCRT_FP64) {
         c->pd->first = first;
         c->pd->count = count;
         c->pd->seed = seed;
-        return launch_f64(c, *c->pd, B, replay, blocks);
+        c->pd->sbins = sb;
+        set_tally_table(c->pd, jm, c->d_copies, tc, c->ncell);
+        rc = launch_f64(c, *c->pd, B, replay, blocks);
+    } else {
+        c->pf->first = first;
+        c->pf->count = count;
+        c->pf->seed = seed;
+        c->pf->sbins = sb;
+        set_tally_table(c->pf, jm, c->d_copies, tc, c->ncell);
+        rc = launch_f32(c, *c->pf, B, replay, blocks);
     }
-    c->pf->first = first;
-    c->pf->count = count;
-    c->pf->seed = seed;
-    return launch_f32(c, *c->pf, B, replay, blocks);
+    if (rc) return rc;
+    if (tc > 1) CK(reduce_tally_copies(jm, c->d_copies, tc - 1, c->ncell, c->nsm, c->stream));
+    return SMCRT_OK;
 }
 
 // Waits for ev1.  The kernel enforces the context's time limit itself (a
@@ -456,6 +538,13 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
         c->stream = opts ? (cudaStream_t)opts->stream : (cudaStream_t)0;
     }
     CKC(cudaMalloc(&c->d_jmean, sizeof(double) * c->ncell));
+    rc = tally_copies(opts, c->ncell, &c->tcopies);
+    if (rc) return bail(rc);
+    if (c->tcopies > 1) {
+        const size_t bytes = sizeof(double) * (size_t)(c->tcopies - 1) * (size_t)c->ncell;
+        CKC(cudaMalloc(&c->d_copies, bytes));
+        CKC(cudaMemset(c->d_copies, 0, bytes));  // the reduce kernel re-zeroes after each launch
+    }
     CKC(cudaMalloc(&c->d_bins, sizeof(double) * std::max(1ll, nbins)));
     CKC(cudaMalloc(&c->d_work, sizeof(unsigned long long) * (1 + C_NUM)));
     CKC(cudaMalloc(&c->d_mom, sizeof(double) * 25));
@@ -473,6 +562,7 @@ void smcrt_destroy(smcrt_ctx* c) {
     if (!c) return;
     cudaStreamSynchronize(c->stream);
     if (c->d_jmean) cudaFree(c->d_jmean);
+    if (c->d_copies) cudaFree(c->d_copies);
     if (c->d_bins) cudaFree(c->d_bins);
     if (c->d_work) cudaFree(c->d_work);
     if (c->d_mom) cudaFree(c->d_mom);
@@ -622,17 +712,13 @@ int run_static_t(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_s
     P.first = first;
     P.count = count;
     P.seed = seed;
+    P.sbins = shared_bins(nbins, count);
+    P.jtab[0] = jmean_dev;  // one fluence grid: no copies without allocation
     int per_sm = 0;
     cudaError_t e;
-    if constexpr (sizeof(R) == 8)
-        e = kern == SMCRT_KERNEL_WEIGHT ? occupancy_f64_1(block, &per_sm)
-          : kern == SMCRT_KERNEL_TEST   ? occupancy_f64_2(block, &per_sm) : occupancy_f64_0(block, &per_sm);
-    else
-        e = kern == SMCRT_KERNEL_WEIGHT ? occupancy_f32_1(block, &per_sm)
-          : kern == SMCRT_KERNEL_TEST   ? occupancy_f32_2(block, &per_sm) : occupancy_f32_0(block, &per_sm);
-    if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
-    if (per_sm < 1) per_sm = 1;
-    if (opts && opts->blocks_per_sm > 0 && opts->blocks_per_sm < per_sm) per_sm = opts->blocks_per_sm;
+    rc = resident_per_sm(sizeof(R) == 8 ? SMCRT_FP64 : SMCRT_FP32, kern, block, sizeof(unsigned) * (size_t)P.sbins,
+                         opts ? opts->blocks_per_sm : 0, &per_sm);
+    if (rc) return rc;
     const long long need = (count + block - 1) / block;
     const int blocks = (int)std::min<long long>((long long)nsm * per_sm, std::max<long long>(need, 1));
     cudaStream_t s = opts ? (cudaStream_t)opts->stream : (cudaStream_t)0;

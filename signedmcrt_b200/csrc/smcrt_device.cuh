@@ -15,6 +15,10 @@ namespace smcrt {
 constexpr int kMaxPrims = 32;
 constexpr int kMaxRegions = 16;
 constexpr int kMaxDetectors = 16;
+// Detector bins privatized per CTA as 32-bit counts in shared memory (16 KiB);
+// larger bin sets (camera images) add straight into the global FP64 bins.
+constexpr int kMaxSharedBins = 4096;
+constexpr int kMaxTallyCopies = 16;
 constexpr double kPI = 3.14159265358979323846264338327950288;
 
 // Device status flags (smcrt_stats.device_status).
@@ -436,6 +440,11 @@ struct Params {
     unsigned int instance;
     long long first;
     long long count;
+    int sbins;    // detector bins counted in shared memory (0: global atomics)
+    int tcopies;                     // fluence-grid copies the CTAs spread their adds over
+    unsigned tmask;                  // tcopies - 1 (tcopies is a power of two)
+    long long ncell;
+    double* jtab[kMaxTallyCopies];   // the grid of each copy; jtab[0] is the output grid
 };
 
 }  // namespace smcrt

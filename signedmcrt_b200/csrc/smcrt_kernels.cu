@@ -12,15 +12,18 @@
 
 namespace smcrt {
 
+// smem: dynamic shared memory of the launch (the privatized detector bins).
 cudaError_t SMCRT_CAT(launch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, const Buffers& B, bool replay, int blocks,
                                                    int block, cudaStream_t s) {
-    if (replay) transport_kernel<SMCRT_R, SMCRT_K, true><<<blocks, block, 0, s>>>(P, B);
-    else transport_kernel<SMCRT_R, SMCRT_K, false><<<blocks, block, 0, s>>>(P, B);
+    const size_t smem = sizeof(unsigned) * (size_t)P.sbins;
+    if (replay) transport_kernel<SMCRT_R, SMCRT_K, true><<<blocks, block, smem, s>>>(P, B);
+    else transport_kernel<SMCRT_R, SMCRT_K, false><<<blocks, block, smem, s>>>(P, B);
     return cudaGetLastError();
 }
 
-cudaError_t SMCRT_CAT(occupancy, SMCRT_TAG, SMCRT_K)(int block, int* per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, transport_kernel<SMCRT_R, SMCRT_K, false>, block, 0);
+cudaError_t SMCRT_CAT(occupancy, SMCRT_TAG, SMCRT_K)(int block, size_t smem, int* per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, transport_kernel<SMCRT_R, SMCRT_K, false>, block,
+                                                         smem);
 }
 
 }  // namespace smcrt

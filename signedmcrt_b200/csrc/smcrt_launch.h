@@ -10,7 +10,7 @@ namespace smcrt {
 #define SMCRT_DECL_VARIANT(R, TAG, K)                                                                       \
     cudaError_t launch_##TAG##_##K(const Params<R>& P, const Buffers& B, bool replay, int blocks, int block, \
                                    cudaStream_t s);                                                       \
-    cudaError_t occupancy_##TAG##_##K(int block, int* per_sm);
+    cudaError_t occupancy_##TAG##_##K(int block, size_t smem, int* per_sm);
 
 SMCRT_DECL_VARIANT(float, f32, 0)
 SMCRT_DECL_VARIANT(float, f32, 1)
@@ -19,6 +19,9 @@ SMCRT_DECL_VARIANT(double, f64, 0)
 SMCRT_DECL_VARIANT(double, f64, 1)
 SMCRT_DECL_VARIANT(double, f64, 2)
 #undef SMCRT_DECL_VARIANT
+
+// Sums `ncopies` fluence-grid copies into `out` and zeroes them (smcrt_api.cu).
+cudaError_t reduce_tally_copies(double* out, double* copies, int ncopies, long long ncell, int nsm, cudaStream_t s);
 
 // Device-function probes (smcrt_probes.cu).
 cudaError_t probe_eval_sdf(int precision, const smcrt_scene* scene, const double* d_pts, long long n, double* d_out);

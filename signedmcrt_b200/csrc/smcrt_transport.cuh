@@ -208,18 +208,32 @@ __device__ __forceinline__ long long detector_bin(const DetT& D, const double p[
     return D.off + idx - 1;
 }
 
-// Detector hits at packet death (kernelsMod.f90:302-306), out of line and by
-// value: it runs once per packet.
+// Detector hits at packet death (kernelsMod.f90:302-306).  Each hit adds one
+// count; with privatized bins the count goes to the CTA's shared-memory copy.
 template <class R>
-__device__ __noinline__ void record_detectors(const Params<R>& P, double* bins, double px, double py, double pz,
-                                              double lx, double ly, double lz, double weight, int layer1) {
+__device__ __forceinline__ void record_detectors(const Params<R>& P, double* bins, unsigned* sbins, double px,
+                                                 double py, double pz, double lx, double ly, double lz,
+                                                 double weight, int layer1) {
     const double p[3] = {px, py, pz};
     const double l[3] = {lx, ly, lz};
     const double value = (P.kernel == SMCRT_KERNEL_WEIGHT) ? weight : sqrt(px * px + py * py);
     for (int d = 0; d < P.ndet; ++d) {
         const long long b = detector_bin(P.det[d], p, l, value, layer1);
-        if (b >= 0) atomicAdd(bins + b, 1.0);
+        if (b >= 0) {
+            if (P.sbins) atomicAdd(sbins + b, 1u);
+            else atomicAdd(bins + b, 1.0);
+        }
     }
+}
+
+// The fluence grid this CTA adds into: copy (CTA index mod tcopies).  The CTA
+// index is read at each use (volatile) rather than kept in a register across the
+// transport loop, and the copy's address comes from the parameter bank.
+template <class R>
+__device__ __forceinline__ double* tally_grid(const Params<R>& P) {
+    unsigned b;
+    asm volatile("mov.u32 %0, %%ctaid.x;" : "=r"(b));
+    return P.jtab[b & P.tmask];
 }
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -264,13 +278,14 @@ struct Flight {
     };
 };
 
-// One region at one point, out of line: used only on rare paths (crossings),
-// so the hot sweep stays the only inlined copy of the primitive switch.
+// Single-region evaluations of the crossing path.  They stay inline: an
+// out-of-line function would receive the parameter block by reference and read
+// it through generic loads instead of the constant bank.
 template <class R>
-__device__ __noinline__ R eval_region_cold(const SceneT<R>& sc, int r, V3<R> p) {
+__device__ __forceinline__ R eval_region_cold(const SceneT<R>& sc, int r, V3<R> p) {
     return eval_region(sc, r, p);
 }
-static __device__ __noinline__ V3<double> calc_normal_cold(const SceneT<double>& sc, int r, V3<double> p, double h) {
+__device__ __forceinline__ V3<double> calc_normal_cold(const SceneT<double>& sc, int r, V3<double> p, double h) {
     return calc_normal(sc, r, p, h);
 }
 
@@ -306,6 +321,8 @@ __device__ __forceinline__ int start_step(const Params<R>& P, const Pk<R>& pk, F
         tflag = true;  // outside the grid: no tally for this step
         return -1;
     }
+    // distance to the first face on each axis, then one face spacing per crossing
+    // (Amanatides & Woo): no division per segment
     const R big = (R)1e30;
     const V3<R>& d = pk.dir;
     f.w.tx = d.x > (R)0 ? fmax(((R)f.w.ci * g.vx - o.x) / d.x, (R)0)
@@ -318,10 +335,18 @@ __device__ __forceinline__ int start_step(const Params<R>& P, const Pk<R>& pk, F
     return A_WALK;
 }
 
+// Distance between successive faces of one axis along the direction.
+template <class R>
+__device__ __forceinline__ R face_spacing(R v, R dcomp) {
+    return v / fabs(dcomp);
+}
+
 // One voxel segment of the current step; returns true when the step's walk is over.
 template <class R>
-__device__ __forceinline__ bool walk_segment(const GridT<R>& g, double* __restrict__ jm, const V3<double>& pos,
-                                             const V3<R>& d, Flight<R>& f, Cnt& c, bool& tflag) {
+__device__ __forceinline__ bool walk_segment(const Params<R>& P, const V3<double>& pos, const V3<R>& d, Flight<R>& f,
+                                             Cnt& c, bool& tflag) {
+    const GridT<R>& g = P.grid;
+    double* const jm = tally_grid(P);
     const R tm = fmin(f.w.tx, fmin(f.w.ty, f.w.tz));
     const int idx = (f.w.ci - 1) + g.nx * ((f.w.cj - 1) + g.ny * (f.w.ck - 1));
     ++c.vox;
@@ -331,22 +356,18 @@ __device__ __forceinline__ bool walk_segment(const GridT<R>& g, double* __restri
     }
     atomicAdd(jm + idx, (double)(tm - f.w.td));
     f.w.td = tm;
-    const V3<R> o = grid_origin(g, pos);
     if (tm == f.w.tx) {
-        const int s = d.x > (R)0 ? 1 : -1;
-        f.w.ci += s;
+        f.w.ci += d.x > (R)0 ? 1 : -1;
         if (f.w.ci < 1 || f.w.ci > g.nx) { tflag = true; return true; }
-        f.w.tx = fmax(((R)(s > 0 ? f.w.ci : f.w.ci - 1) * g.vx - o.x) / d.x, (R)0);
+        f.w.tx = tm + face_spacing(g.vx, d.x);
     } else if (tm == f.w.ty) {
-        const int s = d.y > (R)0 ? 1 : -1;
-        f.w.cj += s;
+        f.w.cj += d.y > (R)0 ? 1 : -1;
         if (f.w.cj < 1 || f.w.cj > g.ny) { tflag = true; return true; }
-        f.w.ty = fmax(((R)(s > 0 ? f.w.cj : f.w.cj - 1) * g.vy - o.y) / d.y, (R)0);
+        f.w.ty = tm + face_spacing(g.vy, d.y);
     } else {
-        const int s = d.z > (R)0 ? 1 : -1;
-        f.w.ck += s;
+        f.w.ck += d.z > (R)0 ? 1 : -1;
         if (f.w.ck < 1 || f.w.ck > g.nz) { tflag = true; return true; }
-        f.w.tz = fmax(((R)(s > 0 ? f.w.ck : f.w.ck - 1) * g.vz - o.z) / d.z, (R)0);
+        f.w.tz = tm + face_spacing(g.vz, d.z);
     }
     return false;
 }
@@ -390,8 +411,10 @@ __global__ void __launch_bounds__(256, SMCRT_MIN_BLOCKS) transport_kernel(const 
                                                                           const Buffers B) {
     __shared__ unsigned long long s_cnt[C_NUM];
     __shared__ double s_mom[25];
+    extern __shared__ unsigned s_bins[];  // P.sbins detector counts
     if (threadIdx.x < C_NUM) s_cnt[threadIdx.x] = 0ull;
     if (threadIdx.x < 25) s_mom[threadIdx.x] = 0.0;
+    for (int i = threadIdx.x; i < P.sbins; i += blockDim.x) s_bins[i] = 0u;
     __syncthreads();
 
     const SceneT<R>& sc = P.sc;
@@ -417,7 +440,7 @@ __global__ void __launch_bounds__(256, SMCRT_MIN_BLOCKS) transport_kernel(const 
         // ---- retire a finished packet: detectors (kernelsMod.f90:302-306), counters
         if (act == A_DEATH) {
             if (P.ndet > 0 && KERNEL != SMCRT_KERNEL_TEST)
-                record_detectors(P, B.bins, pk.pos.x, pk.pos.y, pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
+                record_detectors(P, B.bins, s_bins, pk.pos.x, pk.pos.y, pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
                                  (double)pk.dir.z, (double)pk.weight, pk.layer + 1);
             atomicAdd(&s_cnt[C_PACKETS], 1ull);
             atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);
@@ -487,7 +510,7 @@ __global__ void __launch_bounds__(256, SMCRT_MIN_BLOCKS) transport_kernel(const 
                     pk.tflag = true;
                     act = A_DEATH;
                 } else {
-                    atomicAdd(B.jmean + (ci - 1) + (long long)P.grid.nx * ((cj - 1) + (long long)P.grid.ny * (ck - 1)),
+                    atomicAdd(tally_grid(P) + (ci - 1) + (long long)P.grid.nx * ((cj - 1) + (long long)P.grid.ny * (ck - 1)),
                               (double)wa);
                     pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
                     ++c.scat;
@@ -665,7 +688,7 @@ __global__ void __launch_bounds__(256, SMCRT_MIN_BLOCKS) transport_kernel(const 
         // ---- walk voxel segments: at most SMCRT_WALK_SEGMENTS per lane per
         // iteration, so one long walk does not hold up the other lanes' actions
         for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
-            if (walk_segment(P.grid, B.jmean, pk.pos, pk.dir, f, c, pk.tflag)) {
+            if (walk_segment(P, pk.pos, pk.dir, f, c, pk.tflag)) {
                 pk.pos = advance(pk.pos, f.dsdf, pk.dir);
                 if (f.last) {
                     act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
@@ -679,6 +702,8 @@ __global__ void __launch_bounds__(256, SMCRT_MIN_BLOCKS) transport_kernel(const 
     __syncthreads();
     if (threadIdx.x < C_NUM && s_cnt[threadIdx.x]) atomicAdd(B.counters + threadIdx.x, s_cnt[threadIdx.x]);
     if (threadIdx.x < 25 && s_mom[threadIdx.x] != 0.0) atomicAdd(B.moments + threadIdx.x, s_mom[threadIdx.x]);
+    for (int i = threadIdx.x; i < P.sbins; i += blockDim.x)
+        if (s_bins[i]) atomicAdd(B.bins + i, (double)s_bins[i]);
 }
 
 }  // namespace smcrt

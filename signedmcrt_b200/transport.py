@@ -36,7 +36,7 @@ class Transport:
     def __init__(self, array, settings: Settings, *, kernel: str = "pathlength", precision: str = "fp32",
                  end_early: bool = False, stream: int | None = None, block_size: int = 0, blocks_per_sm: int = 0,
                  eps: float = 0.0, normal_h: float = 0.0, max_trace_steps: int = 0, timeout_ms: int = 0,
-                 instance: int = 0):
+                 instance: int = 0, tally_copies: int = 0):
         self.settings = settings
         self.flat = array if isinstance(array, FlatScene) else FlatScene(array)
         self.grid = settings.grid_c()
@@ -53,6 +53,7 @@ class Transport:
         o.eps, o.normal_h = eps, normal_h
         o.instance = instance
         o.timeout_ms = timeout_ms
+        o.tally_copies = tally_copies  # 0: library choice; 1: a single fluence grid
         # stream=None: a stream private to this context; an int: that cudaStream_t (0 = default)
         o.stream = stream if stream is not None else None
         o.private_stream = int(stream is None)

@@ -62,7 +62,7 @@ STRUCTS = {
     "smcrt_detector": (abi.Detector, ["kind", "layer", "nbins", "pos", "dir", "r1", "r2", "maxval", "p2", "p3"]),
     "smcrt_options": (abi.Options, ["kernel", "precision", "end_early", "block_size", "blocks_per_sm",
                                     "max_trace_steps", "eps", "normal_h", "instance", "timeout_ms", "stream",
-                                    "private_stream"]),
+                                    "private_stream", "tally_copies"]),
     "smcrt_stats": (abi.Stats, ["nscatt", "packets", "sdf_evals", "voxel_segments", "trace_steps", "scatters",
                                 "fresnel_events", "reflections", "kills_step_cap", "kills_error", "rng_draws",
                                 "moments", "kernel_ms", "device_status"]),

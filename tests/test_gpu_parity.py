@@ -365,3 +365,37 @@ def test_invalid_inputs_are_errors(gpu):
     with pytest.raises(_lib.SmcrtError) as e:
         gpu.Transport(P.setup_simulation(st), st)
     assert e.value.code == abi.ERR_ARG
+
+
+def test_tally_copies_sum_to_the_single_grid(gpu):
+    """Fluence-grid copies only spread the atomic adds: the same FP64 histories
+    tallied into 1 or 8 copies give the same counters, bins and fluence."""
+    st = P.benchmark_settings("box_slab")
+    arr = P.setup_simulation(st)
+    out = []
+    for copies in (1, 8):
+        with gpu.Transport(arr, st, precision="fp64", tally_copies=copies) as tr:
+            out.append(tr.run(50000, 17))
+    a, b = out
+    assert all(a.stats[k] == b.stats[k] for k in COUNT_KEYS)
+    # FP64 atomics add in a different order: agreement to accumulated rounding
+    assert np.allclose(a.jmean, b.jmean, rtol=1e-10, atol=1e-12 * a.jmean.max())
+    assert np.array_equal(a.bins, b.bins)
+
+
+@pytest.mark.parametrize("nbins", [40, 70])
+def test_camera_bins_shared_and_global(gpu, oracle, nbins):
+    """A camera of 41^2 bins is counted in shared memory, one of 71^2 bins (above
+    the 4096-bin limit) in the global bins: both equal the oracle's FP64 bins."""
+    from signedmcrt_b200.config import DetectorCfg
+    st = P.benchmark_settings("box_slab")
+    st.detectors = [DetectorCfg("camera", p1=(-1.0, -1.0, -1.0), p2=(1.0, -1.0, -1.0), p3=(-1.0, 1.0, -1.0),
+                                layer=1, nbins=nbins, maxval=2.0)]
+    arr = P.setup_simulation(st)
+    n = 20000
+    with gpu.Transport(arr, st, precision="fp64") as tr:
+        g = tr.run(n, 31)
+    o = oracle.run(arr, st, nphotons=n, seed=31, policy=oracle.device_policy("fp64", st.grid_c()))
+    assert g.bins.size == (nbins + 1) ** 2
+    assert g.bins.sum() > 0
+    assert np.array_equal(g.bins, o.bins)
