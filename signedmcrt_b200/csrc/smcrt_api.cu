@@ -513,10 +513,10 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
     c->kernel = kern;
     c->ncell = (long long)grid->nxg * grid->nyg * grid->nzg;
     c->nbins = nbins;
-    c->block = (opts && opts->block_size > 0) ? opts->block_size : 256;
-    if (c->block > 256 || c->block % 32) {
+    c->block = (opts && opts->block_size > 0) ? opts->block_size : kBlock;
+    if (c->block != kBlock) {
         delete c;
-        return fail(SMCRT_ERR_ARG, "options: block_size must be a multiple of 32 <= 256");
+        return fail(SMCRT_ERR_ARG, "options: block_size must be 0 or " + std::to_string(kBlock));
     }
     c->timeout_ms = (opts && opts->timeout_ms > 0) ? opts->timeout_ms : 600000;
     if (prec == SMCRT_FP64) c->pd = make_params<double>(scene, grid, source, dtab, ndet, opts);
@@ -704,8 +704,8 @@ int run_static_t(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_s
     rc = static_scratch(dev, &scratch);
     if (rc) return rc;
     const int kern = opts ? opts->kernel : SMCRT_KERNEL_PATHLENGTH;
-    const int block = (opts && opts->block_size > 0) ? opts->block_size : 256;
-    if (block > 256 || block % 32) return fail(SMCRT_ERR_ARG, "options: block_size must be a multiple of 32 <= 256");
+    const int block = (opts && opts->block_size > 0) ? opts->block_size : kBlock;
+    if (block != kBlock) return fail(SMCRT_ERR_ARG, "options: block_size must be 0 or " + std::to_string(kBlock));
     // the launch parameters live on this host stack (no heap, no device memory)
     Params<R> P;
     fill_params(&P, scene, grid, source, dtab, ndet, opts);

@@ -12,18 +12,34 @@
 
 namespace smcrt {
 
-// smem: dynamic shared memory of the launch (the privatized detector bins).
+// Dynamic shared memory of a launch: the CTA's packet slots, then the
+// privatized detector bins.  The kernel needs more than the default 48 KiB
+// opt-in limit, set once per kernel.
+template <bool REPLAY>
+static cudaError_t allow_smem() {
+    static const cudaError_t e = cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, REPLAY>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)(slots_bytes<SMCRT_R>() + sizeof(unsigned) * kMaxSharedBins));
+    return e;
+}
+
 cudaError_t SMCRT_CAT(launch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, const Buffers& B, bool replay, int blocks,
                                                    int block, cudaStream_t s) {
-    const size_t smem = sizeof(unsigned) * (size_t)P.sbins;
-    if (replay) transport_kernel<SMCRT_R, SMCRT_K, true><<<blocks, block, smem, s>>>(P, B);
-    else transport_kernel<SMCRT_R, SMCRT_K, false><<<blocks, block, smem, s>>>(P, B);
+    if (block != kBlock) return cudaErrorInvalidConfiguration;
+    const size_t smem = slots_bytes<SMCRT_R>() + sizeof(unsigned) * (size_t)P.sbins;
+    cudaError_t e = replay ? allow_smem<true>() : allow_smem<false>();
+    if (e != cudaSuccess) return e;
+    if (replay) transport_kernel<SMCRT_R, SMCRT_K, true><<<blocks, kBlock, smem, s>>>(P, B);
+    else transport_kernel<SMCRT_R, SMCRT_K, false><<<blocks, kBlock, smem, s>>>(P, B);
     return cudaGetLastError();
 }
 
-cudaError_t SMCRT_CAT(occupancy, SMCRT_TAG, SMCRT_K)(int block, size_t smem, int* per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, transport_kernel<SMCRT_R, SMCRT_K, false>, block,
-                                                         smem);
+cudaError_t SMCRT_CAT(occupancy, SMCRT_TAG, SMCRT_K)(int block, size_t sbins_bytes, int* per_sm) {
+    if (block != kBlock) return cudaErrorInvalidConfiguration;
+    cudaError_t e = allow_smem<false>();
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, transport_kernel<SMCRT_R, SMCRT_K, false>, kBlock,
+                                                         slots_bytes<SMCRT_R>() + sbins_bytes);
 }
 
 }  // namespace smcrt

@@ -399,310 +399,550 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
     return a;
 }
 
-// The persistent kernel.  KERNEL: smcrt_kernel_kind.  REPLAY: injected streams.
-//
-// Each iteration runs the actions in a fixed order -- retire, launch,
-// interact, sweep, cross -- then walks voxel segments until no lane of the warp
-// has a segment left.  A lane can pass through several actions per iteration
-// (interact -> sweep -> walk), and lanes at different depths of their flights
-// stay in step because every phase is short.
+// One pass of the transport state machine for one packet: the actions in a
+// fixed order -- retire, launch, interact, sweep, cross -- then at most
+// SMCRT_WALK_SEGMENTS voxel segments.  A packet can pass through several
+// actions in one pass (retire -> launch -> sweep -> walk, interact -> sweep ->
+// walk, sweep -> cross).  `c` counts this thread's events since its last flush.
 template <class R, int KERNEL, bool REPLAY>
-__global__ void __launch_bounds__(256, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
-                                                                          const Buffers B) {
-    __shared__ unsigned long long s_cnt[C_NUM];
-    __shared__ double s_mom[25];
-    extern __shared__ unsigned s_bins[];  // P.sbins detector counts
-    if (threadIdx.x < C_NUM) s_cnt[threadIdx.x] = 0ull;
-    if (threadIdx.x < 25) s_mom[threadIdx.x] = 0.0;
-    for (int i = threadIdx.x; i < P.sbins; i += blockDim.x) s_bins[i] = 0u;
-    __syncthreads();
-
+__device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers& B, Pk<R>& pk, Flight<R>& f,
+                                               Stream<R, REPLAY>& rng, Cnt& c, int& act, unsigned long long* s_cnt,
+                                               double* s_mom, unsigned* s_bins) {
     const SceneT<R>& sc = P.sc;
     const int N = sc.nregions;
     const R eps = P.eps;
-    Pk<R> pk;
-    pk.tflag = true;
-    pk.layer = 0;
-    Flight<R> f;
-    f.mode = S_LAUNCH;
-    Stream<R, REPLAY> rng;
-    Cnt c = {0, 0, 0, 0, 0, 0};
-    int act = A_NEW;
-    long long pid = 0;
-    unsigned iter = 0;
-    const unsigned long long t0 = P.budget_ns ? global_ns() : 0ull;
-    for (;;) {
-        // device-side time budget: past it, stop and flag ABORTED
-        if (P.budget_ns && ((++iter) & 255u) == 0u && global_ns() - t0 > P.budget_ns) {
-            atomicOr(B.status, STATUS_ABORTED);
-            break;
+    // ---- retire a finished packet: detectors (kernelsMod.f90:302-306), counters
+    if (act == A_DEATH) {
+        if (P.ndet > 0 && KERNEL != SMCRT_KERNEL_TEST)
+            record_detectors(P, B.bins, s_bins, pk.pos.x, pk.pos.y, pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
+                             (double)pk.dir.z, (double)pk.weight, pk.layer + 1);
+        atomicAdd(&s_cnt[C_PACKETS], 1ull);
+        atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);
+        atomicAdd(&s_cnt[C_VOX], (unsigned long long)c.vox);
+        atomicAdd(&s_cnt[C_STEPS], (unsigned long long)c.steps);
+        atomicAdd(&s_cnt[C_SCAT], (unsigned long long)c.scat);
+        atomicAdd(&s_cnt[C_FRES], (unsigned long long)c.fres);
+        atomicAdd(&s_cnt[C_REFL], (unsigned long long)c.refl);
+        atomicAdd(&s_cnt[C_DRAWS], (unsigned long long)rng.ndraws);
+        if (pk.flags & STATUS_STEP_CAP) atomicAdd(&s_cnt[C_STEPCAP], 1ull);
+        if (pk.flags & STATUS_ERROR_STATE) atomicAdd(&s_cnt[C_ERR], 1ull);
+        const int fl = pk.flags | rng.flags;
+        if (fl) atomicOr(B.status, fl);
+        if (KERNEL != SMCRT_KERNEL_WEIGHT) atomicAdd(&s_mom[24], (double)pk.nscatt);
+        if (REPLAY) {
+            smcrt_packet_state& st = B.states[(long long)(((uint64_t)rng.p1 << 32) | rng.p0) - P.first];
+            st.pos[0] = pk.pos.x; st.pos[1] = pk.pos.y; st.pos[2] = pk.pos.z;
+            st.dir[0] = pk.dir.x; st.dir[1] = pk.dir.y; st.dir[2] = pk.dir.z;
+            st.weight = pk.weight;
+            st.layer = pk.layer + 1;
+            st.nscatt = pk.nscatt;
+            st.ndraws = rng.ndraws;
+            st.flags = fl;
         }
-        // ---- retire a finished packet: detectors (kernelsMod.f90:302-306), counters
-        if (act == A_DEATH) {
-            if (P.ndet > 0 && KERNEL != SMCRT_KERNEL_TEST)
-                record_detectors(P, B.bins, s_bins, pk.pos.x, pk.pos.y, pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
-                                 (double)pk.dir.z, (double)pk.weight, pk.layer + 1);
-            atomicAdd(&s_cnt[C_PACKETS], 1ull);
-            atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);
-            atomicAdd(&s_cnt[C_VOX], (unsigned long long)c.vox);
-            atomicAdd(&s_cnt[C_STEPS], (unsigned long long)c.steps);
-            atomicAdd(&s_cnt[C_SCAT], (unsigned long long)c.scat);
-            atomicAdd(&s_cnt[C_FRES], (unsigned long long)c.fres);
-            atomicAdd(&s_cnt[C_REFL], (unsigned long long)c.refl);
-            atomicAdd(&s_cnt[C_DRAWS], (unsigned long long)rng.ndraws);
-            if (pk.flags & STATUS_STEP_CAP) atomicAdd(&s_cnt[C_STEPCAP], 1ull);
-            if (pk.flags & STATUS_ERROR_STATE) atomicAdd(&s_cnt[C_ERR], 1ull);
-            const int fl = pk.flags | rng.flags;
-            if (fl) atomicOr(B.status, fl);
-            if (KERNEL != SMCRT_KERNEL_WEIGHT) atomicAdd(&s_mom[24], (double)pk.nscatt);
+        c = Cnt{0, 0, 0, 0, 0, 0};
+        act = A_NEW;
+    }
+    // ---- take the next packet id (warp-aggregated) and emit it
+    if (act == A_NEW) {
+        const unsigned m = __activemask();
+        const unsigned lane = lane_id();
+        const int leader = __ffs(m) - 1;
+        const unsigned rank = __popc(m & ((1u << lane) - 1u));
+        unsigned long long base = 0;
+        if ((int)lane == leader) base = atomicAdd(B.work, (unsigned long long)__popc(m));
+        base = __shfl_sync(m, base, leader);
+        const long long pid = (long long)(base + rank);
+        if (pid >= P.count) {
+            act = A_DONE;
+        } else {
+            const long long gpid = P.first + pid;
             if (REPLAY) {
-                smcrt_packet_state& st = B.states[pid];
-                st.pos[0] = pk.pos.x; st.pos[1] = pk.pos.y; st.pos[2] = pk.pos.z;
-                st.dir[0] = pk.dir.x; st.dir[1] = pk.dir.y; st.dir[2] = pk.dir.z;
-                st.weight = pk.weight;
-                st.layer = pk.layer + 1;
-                st.nscatt = pk.nscatt;
-                st.ndraws = rng.ndraws;
-                st.flags = fl;
-            }
-            c = Cnt{0, 0, 0, 0, 0, 0};
-            act = A_NEW;
-        }
-        // ---- take the next packet id (warp-aggregated) and emit it
-        if (act == A_NEW) {
-            const unsigned m = __activemask();
-            const unsigned lane = lane_id();
-            const int leader = __ffs(m) - 1;
-            const unsigned rank = __popc(m & ((1u << lane) - 1u));
-            unsigned long long base = 0;
-            if ((int)lane == leader) base = atomicAdd(B.work, (unsigned long long)__popc(m));
-            base = __shfl_sync(m, base, leader);
-            pid = (long long)(base + rank);
-            if (pid >= P.count) {
-                act = A_DONE;
+                const long long o0 = B.offsets[pid], o1 = B.offsets[pid + 1];
+                rng.init(P.seed, P.instance, (uint64_t)gpid, B.uniforms + o0, (int)(o1 - o0));
             } else {
-                const long long gpid = P.first + pid;
-                if (REPLAY) {
-                    const long long o0 = B.offsets[pid], o1 = B.offsets[pid + 1];
-                    rng.init(P.seed, P.instance, (uint64_t)gpid, B.uniforms + o0, (int)(o1 - o0));
-                } else {
-                    rng.init(P.seed, P.instance, (uint64_t)gpid, nullptr, 0);
-                }
-                emit(P, pk, rng);
-                start_flight(f, rng);
-                f.mode = S_LAUNCH;
-                act = A_SWEEP;
+                rng.init(P.seed, P.instance, (uint64_t)gpid, nullptr, 0);
             }
-        }
-        if (act == A_DONE) break;
-        // ---- between flights (kernelsMod.f90:285-300 / 99-134 / 408-436)
-        if (act == A_INTERACT) {
-            const DRegion<R>& rg = sc.region[pk.layer];
+            emit(P, pk, rng);
+            start_flight(f, rng);
+            f.mode = S_LAUNCH;
             act = A_SWEEP;
-            if (KERNEL == SMCRT_KERNEL_WEIGHT) {
-                const R wa = pk.weight * ((R)1 - rg.albedo);
-                pk.weight = pk.weight - wa;
-                const R ox = (R)pk.pos.x + P.grid.xmax, oy = (R)pk.pos.y + P.grid.ymax, oz = (R)pk.pos.z + P.grid.zmax;
-                const int ci = (int)floor((R)P.grid.nx * ox / ((R)2 * P.grid.xmax)) + 1;
-                const int cj = (int)floor((R)P.grid.ny * oy / ((R)2 * P.grid.ymax)) + 1;
-                const int ck = (int)floor((R)P.grid.nz * oz / ((R)2 * P.grid.zmax)) + 1;
-                if (ci < 1 || ci > P.grid.nx || cj < 1 || cj > P.grid.ny || ck < 1 || ck > P.grid.nz) {
-                    pk.tflag = true;
-                    act = A_DEATH;
-                } else {
-                    atomicAdd(tally_grid(P) + (ci - 1) + (long long)P.grid.nx * ((cj - 1) + (long long)P.grid.ny * (ck - 1)),
-                              (double)wa);
-                    pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
-                    ++c.scat;
-                    if (pk.weight < (R)0.01) {  // THRESHOLD, CHANCE (constants.f90:28-30)
-                        if (rng.next() < (R)0.1) pk.weight = pk.weight / (R)0.1;
-                        else {
-                            pk.tflag = true;
-                            act = A_DEATH;
-                        }
-                    }
-                }
+        }
+    }
+    if (act == A_DONE) return;
+    // ---- between flights (kernelsMod.f90:285-300 / 99-134 / 408-436)
+    if (act == A_INTERACT) {
+        const DRegion<R>& rg = sc.region[pk.layer];
+        act = A_SWEEP;
+        if (KERNEL == SMCRT_KERNEL_WEIGHT) {
+            const R wa = pk.weight * ((R)1 - rg.albedo);
+            pk.weight = pk.weight - wa;
+            const R ox = (R)pk.pos.x + P.grid.xmax, oy = (R)pk.pos.y + P.grid.ymax, oz = (R)pk.pos.z + P.grid.zmax;
+            const int ci = (int)floor((R)P.grid.nx * ox / ((R)2 * P.grid.xmax)) + 1;
+            const int cj = (int)floor((R)P.grid.ny * oy / ((R)2 * P.grid.ymax)) + 1;
+            const int ck = (int)floor((R)P.grid.nz * oz / ((R)2 * P.grid.zmax)) + 1;
+            if (ci < 1 || ci > P.grid.nx || cj < 1 || cj > P.grid.ny || ck < 1 || ck > P.grid.nz) {
+                pk.tflag = true;
+                act = A_DEATH;
             } else {
-                const R ran = rng.next();
-                if (ran < rg.albedo) {
-                    pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
-                    ++c.scat;
-                    pk.nscatt += 1;
-                    if (KERNEL == SMCRT_KERNEL_TEST) {
-                        const int sidx = pk.nscatt;
-                        if (sidx >= 1 && sidx <= 4) {
-                            const double px = pk.pos.x, py = pk.pos.y, pz = pk.pos.z;
-                            atomicAdd(&s_mom[(sidx - 1) * 3 + 0], px);
-                            atomicAdd(&s_mom[(sidx - 1) * 3 + 1], py);
-                            atomicAdd(&s_mom[(sidx - 1) * 3 + 2], pz);
-                            atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 0], px * px);
-                            atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 1], py * py);
-                            atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 2], pz * pz);
-                        } else if (P.end_early) {
-                            pk.tflag = true;  // the reference still calls tauint2 once more (:428-435)
-                        }
-                    }
-                } else {
-                    pk.tflag = true;
-                    act = A_DEATH;
-                }
-            }
-            if (act == A_SWEEP) {
-                start_flight(f, rng);
-                f.mode = S_TOP;
-            }
-        }
-        // ---- evaluate every region at the current position (the one inlined sweep)
-        if (act == A_SWEEP) {
-            const V3<R> pf = cv<R>(pk.pos);
-            const int L = pk.layer;
-            R mn = (R)INFINITY, mna = (R)INFINITY, inner = (R)INFINITY;
-            R d0 = 0, dsL = 0, dsN = 0;
-            int nl = -1, lay = 0;
-            for (int i = 0; i < N; ++i) {
-                const R d = eval_region(sc, i, pf);
-                mn = fmin(mn, d);
-                mna = fmin(mna, fabs(d));
-                if (i == 0) d0 = d;
-                if (i == L) dsL = d;
-                if (nl < 0 && d < (R)0) {
-                    nl = i;
-                    dsN = d;
-                }
-                // launch layer (kernelsMod.f90:275-280): innermost containing region
-                const R a = (d > (R)0) ? (R)999.0 : fabs(d);
-                if (a < inner) {
-                    inner = a;
-                    lay = i;
-                }
-            }
-            c.sdf += N;
-            f.dsdf = mna;
-            const int mode = f.mode;
-            if (mode == S_LAUNCH || mode == S_TOP) {
-                // top of tauint2's outer loop (:51-61).  At launch the same sweep also
-                // gives the layer (the reference evaluates the same point twice).
-                if (mode == S_LAUNCH) {
-                    pk.layer = lay;
-                    c.sdf += N;
-                }
-                f.steps = 0;
-                // d == eps (reachable on the FP32 coordinate grid) counts as on the
-                // surface, like the reflected packets the reference kills here
-                if (mna <= eps) {
-                    pk.tflag = true;
-                    act = end_flight(P, pk);
-                } else {
-                    act = step_or_skip(P, pk, f, c);
-                }
-            } else if (mode == S_STEP) {
-                if (mn >= (R)0) {  // outside every region (:92-96)
-                    pk.tflag = true;
-                    act = end_flight(P, pk);
-                } else if (++f.steps >= P.max_steps) {
-                    pk.tflag = true;
-                    pk.flags |= STATUS_STEP_CAP;
-                    act = end_flight(P, pk);
-                } else if (mna > eps) {
-                    act = step_or_skip(P, pk, f, c);
-                } else if (f.taurun >= f.tau || pk.tflag) {
-                    act = end_flight(P, pk);  // (:99-102)
-                } else {
-                    // surface reached: count the reference's dstmp sweep (values of this
-                    // one, :104-108) and take the crossing step of min|d| + 2 eps
-                    c.sdf += N;
-                    f.x.oldpos = pk.pos;
-                    pk.pos = advance(pk.pos, mna + (R)2 * eps, pk.dir);
-                    f.mode = S_CROSS;
-                    act = A_SWEEP + 100;  // sweep again at the new position (next iteration)
-                }
-            } else {  // S_CROSS: sweep at the stepped position (:117-184)
-                if (nl < 0) {
-                    nl = 0;
-                    dsN = d0;
-                }
-                act = A_CROSS;
-                f.mode = S_TOP;
-                if (sc.region[L].nidx != sc.region[nl].nidx) {
-                    int which = -1;
-                    if (dsL < (R)0 && dsN < (R)0) {
-                        which = (fabs(dsL) <= fabs(dsN)) ? L : nl;
-                    } else {
-                        const V3<R> of = cv<R>(f.x.oldpos);
-                        const R tL = eval_region_cold(sc, L, of), tN = eval_region_cold(sc, nl, of);
-                        if (tL < (R)0 && tN < (R)0) {
-                            which = (tL >= tN) ? L : nl;
-                        } else if (dsL >= (R)0 && dsN < (R)0) {
-                            // exactly 0 counts as outside, like the `ds(i) < 0` membership
-                            // test; the `error stop` branch (:155-156) is then reached only by NaN
-                            which = (L == 0) ? L : nl;  // oldlayer = packet%layer, then "== 1" (:150-162)
-                        } else if (dsL >= (R)0 && dsN >= (R)0) {
-                            pk.tflag = true;
-                        } else {
-                            pk.tflag = true;
-                            pk.flags |= STATUS_ERROR_STATE;
-                        }
-                    }
-                    f.x.which = which;  // the boundary event runs in the A_CROSS phase below
-                    f.x.nl = nl;
-                } else {
-                    pk.layer = nl;
-                    f.x.which = -2;  // same refractive index: continue with the same tau
-                }
-                if (pk.tflag) act = end_flight(P, pk);
-            }
-        }
-        if (act == A_SWEEP + 100) act = A_SWEEP;
-        // ---- boundary event in FP64: calcNormal + reflect_refract (surfaces.f90:14-40)
-        if (act == A_CROSS) {
-            act = A_SWEEP;
-            const int which = f.x.which;
-            if (which >= 0) {
-                const int L = pk.layer, nl = f.x.nl;
-                ++c.fres;
-                c.sdf += 4;
-                const V3<double> Nn = calc_normal_cold(P.sc64, which, pk.pos, P.normal_h);
-                V3<double> I{(double)pk.dir.x, (double)pk.dir.y, (double)pk.dir.z};
-                const double m1 = P.sc64.region[L].nidx, m2 = P.sc64.region[nl].nidx;
-                const double Rf = fresnel(I, Nn, m1, m2);
-                const double u = (double)rng.next();
-                const bool refl = u <= Rf;
-                I = refl ? reflect(I, Nn) : refract(I, Nn, m1 / m2);
-                pk.dir = V3<R>{(R)I.x, (R)I.y, (R)I.z};
-                pk.weight = pk.weight * (R)Rf;
-                f.tau = -log(rng.next());
-                f.taurun = 0;
-                if (!refl) {
-                    pk.layer = nl;
-                } else {
-                    ++c.refl;
-                    pk.pos = f.x.oldpos;
-                    pk.bounces += 1;
-                    if (pk.bounces > 1000) {
+                atomicAdd(tally_grid(P) + (ci - 1) + (long long)P.grid.nx * ((cj - 1) + (long long)P.grid.ny * (ck - 1)),
+                          (double)wa);
+                pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
+                ++c.scat;
+                if (pk.weight < (R)0.01) {  // THRESHOLD, CHANCE (constants.f90:28-30)
+                    if (rng.next() < (R)0.1) pk.weight = pk.weight / (R)0.1;
+                    else {
                         pk.tflag = true;
-                        act = end_flight(P, pk);
+                        act = A_DEATH;
                     }
                 }
             }
+        } else {
+            const R ran = rng.next();
+            if (ran < rg.albedo) {
+                pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
+                ++c.scat;
+                pk.nscatt += 1;
+                if (KERNEL == SMCRT_KERNEL_TEST) {
+                    const int sidx = pk.nscatt;
+                    if (sidx >= 1 && sidx <= 4) {
+                        const double px = pk.pos.x, py = pk.pos.y, pz = pk.pos.z;
+                        atomicAdd(&s_mom[(sidx - 1) * 3 + 0], px);
+                        atomicAdd(&s_mom[(sidx - 1) * 3 + 1], py);
+                        atomicAdd(&s_mom[(sidx - 1) * 3 + 2], pz);
+                        atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 0], px * px);
+                        atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 1], py * py);
+                        atomicAdd(&s_mom[12 + (sidx - 1) * 3 + 2], pz * pz);
+                    } else if (P.end_early) {
+                        pk.tflag = true;  // the reference still calls tauint2 once more (:428-435)
+                    }
+                }
+            } else {
+                pk.tflag = true;
+                act = A_DEATH;
+            }
         }
-        // ---- walk voxel segments: at most SMCRT_WALK_SEGMENTS per lane per
-        // iteration, so one long walk does not hold up the other lanes' actions
-        for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
-            if (walk_segment(P, pk.pos, pk.dir, f, c, pk.tflag)) {
-                pk.pos = advance(pk.pos, f.dsdf, pk.dir);
-                if (f.last) {
-                    act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
+        if (act == A_SWEEP) {
+            start_flight(f, rng);
+            f.mode = S_TOP;
+        }
+    }
+    // ---- evaluate every region at the current position (the one inlined sweep)
+    if (act == A_SWEEP) {
+        const V3<R> pf = cv<R>(pk.pos);
+        const int L = pk.layer;
+        R mn = (R)INFINITY, mna = (R)INFINITY, inner = (R)INFINITY;
+        R d0 = 0, dsL = 0, dsN = 0;
+        int nl = -1, lay = 0;
+        for (int i = 0; i < N; ++i) {
+            const R d = eval_region(sc, i, pf);
+            mn = fmin(mn, d);
+            mna = fmin(mna, fabs(d));
+            if (i == 0) d0 = d;
+            if (i == L) dsL = d;
+            if (nl < 0 && d < (R)0) {
+                nl = i;
+                dsN = d;
+            }
+            // launch layer (kernelsMod.f90:275-280): innermost containing region
+            const R a = (d > (R)0) ? (R)999.0 : fabs(d);
+            if (a < inner) {
+                inner = a;
+                lay = i;
+            }
+        }
+        c.sdf += N;
+        f.dsdf = mna;
+        const int mode = f.mode;
+        if (mode == S_LAUNCH || mode == S_TOP) {
+            // top of tauint2's outer loop (:51-61).  At launch the same sweep also
+            // gives the layer (the reference evaluates the same point twice).
+            if (mode == S_LAUNCH) {
+                pk.layer = lay;
+                c.sdf += N;
+            }
+            f.steps = 0;
+            // d == eps (reachable on the FP32 coordinate grid) counts as on the
+            // surface, like the reflected packets the reference kills here
+            if (mna <= eps) {
+                pk.tflag = true;
+                act = end_flight(P, pk);
+            } else {
+                act = step_or_skip(P, pk, f, c);
+            }
+        } else if (mode == S_STEP) {
+            if (mn >= (R)0) {  // outside every region (:92-96)
+                pk.tflag = true;
+                act = end_flight(P, pk);
+            } else if (++f.steps >= P.max_steps) {
+                pk.tflag = true;
+                pk.flags |= STATUS_STEP_CAP;
+                act = end_flight(P, pk);
+            } else if (mna > eps) {
+                act = step_or_skip(P, pk, f, c);
+            } else if (f.taurun >= f.tau || pk.tflag) {
+                act = end_flight(P, pk);  // (:99-102)
+            } else {
+                // surface reached: count the reference's dstmp sweep (values of this
+                // one, :104-108) and take the crossing step of min|d| + 2 eps
+                c.sdf += N;
+                f.x.oldpos = pk.pos;
+                pk.pos = advance(pk.pos, mna + (R)2 * eps, pk.dir);
+                f.mode = S_CROSS;
+                act = A_SWEEP + 100;  // sweep again at the new position (next iteration)
+            }
+        } else {  // S_CROSS: sweep at the stepped position (:117-184)
+            if (nl < 0) {
+                nl = 0;
+                dsN = d0;
+            }
+            act = A_CROSS;
+            f.mode = S_TOP;
+            if (sc.region[L].nidx != sc.region[nl].nidx) {
+                int which = -1;
+                if (dsL < (R)0 && dsN < (R)0) {
+                    which = (fabs(dsL) <= fabs(dsN)) ? L : nl;
                 } else {
-                    f.mode = S_STEP;
-                    act = A_SWEEP;
+                    const V3<R> of = cv<R>(f.x.oldpos);
+                    const R tL = eval_region_cold(sc, L, of), tN = eval_region_cold(sc, nl, of);
+                    if (tL < (R)0 && tN < (R)0) {
+                        which = (tL >= tN) ? L : nl;
+                    } else if (dsL >= (R)0 && dsN < (R)0) {
+                        // exactly 0 counts as outside, like the `ds(i) < 0` membership
+                        // test; the `error stop` branch (:155-156) is then reached only by NaN
+                        which = (L == 0) ? L : nl;  // oldlayer = packet%layer, then "== 1" (:150-162)
+                    } else if (dsL >= (R)0 && dsN >= (R)0) {
+                        pk.tflag = true;
+                    } else {
+                        pk.tflag = true;
+                        pk.flags |= STATUS_ERROR_STATE;
+                    }
+                }
+                f.x.which = which;  // the boundary event runs in the A_CROSS phase below
+                f.x.nl = nl;
+            } else {
+                pk.layer = nl;
+                f.x.which = -2;  // same refractive index: continue with the same tau
+            }
+            if (pk.tflag) act = end_flight(P, pk);
+        }
+    }
+    if (act == A_SWEEP + 100) act = A_SWEEP;
+    // ---- boundary event in FP64: calcNormal + reflect_refract (surfaces.f90:14-40)
+    if (act == A_CROSS) {
+        act = A_SWEEP;
+        const int which = f.x.which;
+        if (which >= 0) {
+            const int L = pk.layer, nl = f.x.nl;
+            ++c.fres;
+            c.sdf += 4;
+            const V3<double> Nn = calc_normal_cold(P.sc64, which, pk.pos, P.normal_h);
+            V3<double> I{(double)pk.dir.x, (double)pk.dir.y, (double)pk.dir.z};
+            const double m1 = P.sc64.region[L].nidx, m2 = P.sc64.region[nl].nidx;
+            const double Rf = fresnel(I, Nn, m1, m2);
+            const double u = (double)rng.next();
+            const bool refl = u <= Rf;
+            I = refl ? reflect(I, Nn) : refract(I, Nn, m1 / m2);
+            pk.dir = V3<R>{(R)I.x, (R)I.y, (R)I.z};
+            pk.weight = pk.weight * (R)Rf;
+            f.tau = -log(rng.next());
+            f.taurun = 0;
+            if (!refl) {
+                pk.layer = nl;
+            } else {
+                ++c.refl;
+                pk.pos = f.x.oldpos;
+                pk.bounces += 1;
+                if (pk.bounces > 1000) {
+                    pk.tflag = true;
+                    act = end_flight(P, pk);
                 }
             }
         }
     }
+    // ---- walk voxel segments: at most SMCRT_WALK_SEGMENTS per lane per
+    // iteration, so one long walk does not hold up the other lanes' actions
+    for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
+        if (walk_segment(P, pk.pos, pk.dir, f, c, pk.tflag)) {
+            pk.pos = advance(pk.pos, f.dsdf, pk.dir);
+            if (f.last) {
+                act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
+            } else {
+                f.mode = S_STEP;
+                act = A_SWEEP;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Packet slots of one CTA in shared memory (structure of arrays).  Between
+// passes a packet is one slot; the union of the flight record is live only in
+// two states (a voxel walk in progress; a crossing sweep pending) and is stored
+// as raw 32-bit words.
+#ifndef SMCRT_SLOTS_PER_THREAD
+#define SMCRT_SLOTS_PER_THREAD 2
+#endif
+constexpr int kBlock = 256;
+constexpr int kSlots = kBlock * SMCRT_SLOTS_PER_THREAD;
+constexpr int kGroups = 6;  // act values that are sorted (A_NEW .. A_DEATH)
+
+template <class R>
+struct Slots {
+    static constexpr int kRW = sizeof(R) / 4;  // 32-bit words per R
+    static constexpr int kUW = 4 * kRW + 3 > 8 ? 4 * kRW + 3 : 8;  // union words
+    double px[kSlots], py[kSlots], pz[kSlots];
+    R dx[kSlots], dy[kSlots], dz[kSlots], w[kSlots];
+    R tau[kSlots], taurun[kSlots], dsdf[kSlots];
+    uint32_t u[kUW][kSlots];
+    // act | layer << 3 | mode << 7 | last << 9 | tflag << 10 | pk.flags << 16 | rng.flags << 24
+    uint32_t meta[kSlots];
+    int steps[kSlots], nscatt[kSlots];
+    uint32_t bl[kSlots];  // bounces | rng.left << 16
+    uint32_t p0[kSlots], p1[kSlots], block[kSlots], ndraws[kSlots];
+    uint32_t b0[kSlots], b1[kSlots], b2[kSlots], b3[kSlots];
+};
+
+template <class R>
+__device__ __forceinline__ void put_r(uint32_t (*u)[kSlots], int k, int s, R v) {
+    if (sizeof(R) == 4) {
+        u[k][s] = __float_as_uint((float)v);
+    } else {
+        const unsigned long long b = (unsigned long long)__double_as_longlong((double)v);
+        u[k][s] = (uint32_t)b;
+        u[k + 1][s] = (uint32_t)(b >> 32);
+    }
+}
+template <class R>
+__device__ __forceinline__ R get_r(const uint32_t (*u)[kSlots], int k, int s) {
+    if (sizeof(R) == 4) return (R)__uint_as_float(u[k][s]);
+    return (R)__longlong_as_double((long long)(((unsigned long long)u[k + 1][s] << 32) | u[k][s]));
+}
+
+template <class R, bool REPLAY>
+__device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params<R>& P, const Buffers& B, Pk<R>& pk,
+                                         Flight<R>& f, Stream<R, REPLAY>& rng) {
+    const uint32_t m = sl.meta[s];
+    const int act = (int)(m & 7u);
+    pk.layer = (int)((m >> 3) & 15u);
+    f.mode = (int)((m >> 7) & 3u);
+    f.last = (m >> 9) & 1u;
+    pk.tflag = (m >> 10) & 1u;
+    pk.flags = (int)((m >> 16) & 255u);
+    rng.flags = (int)(m >> 24);
+    if (act == A_NEW) return act;
+    pk.pos = V3<double>{sl.px[s], sl.py[s], sl.pz[s]};
+    pk.dir = V3<R>{sl.dx[s], sl.dy[s], sl.dz[s]};
+    pk.weight = sl.w[s];
+    f.tau = sl.tau[s];
+    f.taurun = sl.taurun[s];
+    f.dsdf = sl.dsdf[s];
+    f.steps = sl.steps[s];
+    pk.nscatt = sl.nscatt[s];
+    const uint32_t bl = sl.bl[s];
+    pk.bounces = (int)(bl & 0xFFFFu);
+    rng.left = (int)(bl >> 16);
+    rng.p0 = sl.p0[s];
+    rng.p1 = sl.p1[s];
+    rng.block = sl.block[s];
+    rng.ndraws = (int)sl.ndraws[s];
+    rng.b0 = sl.b0[s];
+    rng.b1 = sl.b1[s];
+    rng.b2 = sl.b2[s];
+    rng.b3 = sl.b3[s];
+    rng.seed = P.seed;
+    rng.inst = P.instance;
+    if (REPLAY) {
+        const long long pid = (long long)(((uint64_t)rng.p1 << 32) | rng.p0) - P.first;
+        const long long o0 = B.offsets[pid], o1 = B.offsets[pid + 1];
+        rng.inj = B.uniforms + o0;
+        rng.ninj = (int)(o1 - o0);
+    }
+    constexpr int W = Slots<R>::kRW;
+    if (act == A_WALK) {
+        f.w.tx = get_r<R>(sl.u, 0, s);
+        f.w.ty = get_r<R>(sl.u, W, s);
+        f.w.tz = get_r<R>(sl.u, 2 * W, s);
+        f.w.td = get_r<R>(sl.u, 3 * W, s);
+        f.w.ci = (int)sl.u[4 * W][s];
+        f.w.cj = (int)sl.u[4 * W + 1][s];
+        f.w.ck = (int)sl.u[4 * W + 2][s];
+    } else if (act == A_SWEEP && f.mode == S_CROSS) {
+        f.x.oldpos.x = get_r<double>(sl.u, 0, s);
+        f.x.oldpos.y = get_r<double>(sl.u, 2, s);
+        f.x.oldpos.z = get_r<double>(sl.u, 4, s);
+        f.x.which = (int)sl.u[6][s];
+        f.x.nl = (int)sl.u[7][s];
+    }
+    return act;
+}
+
+template <class R, bool REPLAY>
+__device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const Pk<R>& pk, const Flight<R>& f,
+                                           const Stream<R, REPLAY>& rng) {
+    sl.meta[s] = (uint32_t)act | ((uint32_t)pk.layer << 3) | ((uint32_t)f.mode << 7) | ((uint32_t)f.last << 9) |
+                 ((uint32_t)pk.tflag << 10) | ((uint32_t)pk.flags << 16) | ((uint32_t)rng.flags << 24);
+    if (act == A_DONE) return;
+    sl.px[s] = pk.pos.x;
+    sl.py[s] = pk.pos.y;
+    sl.pz[s] = pk.pos.z;
+    sl.dx[s] = pk.dir.x;
+    sl.dy[s] = pk.dir.y;
+    sl.dz[s] = pk.dir.z;
+    sl.w[s] = pk.weight;
+    sl.tau[s] = f.tau;
+    sl.taurun[s] = f.taurun;
+    sl.dsdf[s] = f.dsdf;
+    sl.steps[s] = f.steps;
+    sl.nscatt[s] = pk.nscatt;
+    sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 16);
+    sl.p0[s] = rng.p0;
+    sl.p1[s] = rng.p1;
+    sl.block[s] = rng.block;
+    sl.ndraws[s] = (uint32_t)rng.ndraws;
+    sl.b0[s] = rng.b0;
+    sl.b1[s] = rng.b1;
+    sl.b2[s] = rng.b2;
+    sl.b3[s] = rng.b3;
+    constexpr int W = Slots<R>::kRW;
+    if (act == A_WALK) {
+        put_r<R>(sl.u, 0, s, f.w.tx);
+        put_r<R>(sl.u, W, s, f.w.ty);
+        put_r<R>(sl.u, 2 * W, s, f.w.tz);
+        put_r<R>(sl.u, 3 * W, s, f.w.td);
+        sl.u[4 * W][s] = (uint32_t)f.w.ci;
+        sl.u[4 * W + 1][s] = (uint32_t)f.w.cj;
+        sl.u[4 * W + 2][s] = (uint32_t)f.w.ck;
+    } else if (act == A_SWEEP && f.mode == S_CROSS) {
+        put_r<double>(sl.u, 0, s, f.x.oldpos.x);
+        put_r<double>(sl.u, 2, s, f.x.oldpos.y);
+        put_r<double>(sl.u, 4, s, f.x.oldpos.z);
+        sl.u[6][s] = (uint32_t)f.x.which;
+        sl.u[7][s] = (uint32_t)f.x.nl;
+    }
+}
+
+// Dynamic shared memory of one CTA: the slots, then the privatized detector bins.
+template <class R>
+__host__ __device__ constexpr size_t slots_bytes() {
+    return (sizeof(Slots<R>) + 15) / 16 * 16;
+}
+
+// The persistent, compacted kernel.  KERNEL: smcrt_kernel_kind.  REPLAY:
+// injected streams.
+//
+// A CTA holds kSlots packets in shared memory.  Each round it counting-sorts
+// its live slots by their next action (warp ballots, stable in slot order), then
+// every thread takes items t, t + kBlock, ... of the sorted list, runs one pass
+// of the packet's state machine and writes the packet back.  A warp therefore
+// works on 32 packets that start the pass with the same action, whatever mix of
+// actions the CTA's packets are in; rare actions (boundary events, retire and
+// launch) are gathered across the CTA instead of stalling 31 idle lanes.
+template <class R, int KERNEL, bool REPLAY>
+__global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
+                                                                             const Buffers B) {
+    constexpr int Q = SMCRT_SLOTS_PER_THREAD;
+    constexpr int NW = kBlock / 32;
+    __shared__ unsigned long long s_cnt[C_NUM];
+    __shared__ double s_mom[25];
+    __shared__ int s_off[kGroups][Q][NW];
+    __shared__ unsigned short s_list[kSlots];
+    __shared__ int s_total, s_stop;
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    Slots<R>& sl = *reinterpret_cast<Slots<R>*>(s_dyn);
+    unsigned* s_bins = reinterpret_cast<unsigned*>(s_dyn + slots_bytes<R>());
+    const int t = threadIdx.x;
+    const unsigned lane = lane_id();
+    const int warp = t >> 5;
+    if (t < C_NUM) s_cnt[t] = 0ull;
+    if (t < 25) s_mom[t] = 0.0;
+    for (int i = t; i < P.sbins; i += kBlock) s_bins[i] = 0u;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) sl.meta[t + q * kBlock] = (uint32_t)A_NEW;
+
+    Pk<R> pk;
+    Flight<R> f;
+    Stream<R, REPLAY> rng;
+    Cnt c = {0, 0, 0, 0, 0, 0};
+    const unsigned long long t0 = P.budget_ns ? global_ns() : 0ull;
+    const unsigned lt = (1u << lane) - 1u;
+    for (;;) {
+        __syncthreads();  // the previous round's slot writes are visible
+        // ---- sort the live slots by action: per-warp counts and ranks
+        int a[Q], rank[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            a[q] = (int)(sl.meta[t + q * kBlock] & 7u);
+            rank[q] = 0;
+#pragma unroll
+            for (int g = 0; g < kGroups; ++g) {
+                const unsigned m = __ballot_sync(0xffffffffu, a[q] == g);
+                if (a[q] == g) rank[q] = __popc(m & lt);
+                if (lane == 0) s_off[g][q][warp] = __popc(m);
+            }
+        }
+        __syncthreads();
+        // exclusive scan over (group, q, warp): each group contiguous, slot order inside
+        if (warp == 0) {
+            constexpr int E = kGroups * Q * NW;
+            constexpr int PER = (E + 31) / 32;
+            int* flat = &s_off[0][0][0];
+            int v[PER], sum = 0;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int e = (int)lane * PER + k;
+                v[k] = e < E ? flat[e] : 0;
+                sum += v[k];
+            }
+            int incl = sum;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, d);
+                if ((int)lane >= d) incl += y;
+            }
+            int run = incl - sum;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int e = (int)lane * PER + k;
+                if (e < E) flat[e] = run;
+                run += v[k];
+            }
+            if (lane == 31) {
+                s_total = incl;
+                // device-side time budget: past it, stop and flag ABORTED
+                int stop = 0;
+                if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
+                    atomicOr(B.status, STATUS_ABORTED);
+                    stop = 1;
+                }
+                s_stop = stop;
+            }
+        }
+        __syncthreads();
+        const int total = s_total;
+        if (total == 0 || s_stop) break;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (a[q] < kGroups) s_list[s_off[a[q]][q][warp] + rank[q]] = (unsigned short)(t + q * kBlock);
+        __syncthreads();
+        // ---- one pass per listed packet
+        for (int i = t; i < total; i += kBlock) {
+            const int s = s_list[i];
+            int act = load_slot(sl, s, P, B, pk, f, rng);
+            transport_pass<R, KERNEL, REPLAY>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins);
+            store_slot(sl, s, act, pk, f, rng);
+        }
+    }
+    // events of packets still in flight (time budget) and since the last retire
+    atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);
+    atomicAdd(&s_cnt[C_VOX], (unsigned long long)c.vox);
+    atomicAdd(&s_cnt[C_STEPS], (unsigned long long)c.steps);
+    atomicAdd(&s_cnt[C_SCAT], (unsigned long long)c.scat);
+    atomicAdd(&s_cnt[C_FRES], (unsigned long long)c.fres);
+    atomicAdd(&s_cnt[C_REFL], (unsigned long long)c.refl);
     __syncthreads();
-    if (threadIdx.x < C_NUM && s_cnt[threadIdx.x]) atomicAdd(B.counters + threadIdx.x, s_cnt[threadIdx.x]);
-    if (threadIdx.x < 25 && s_mom[threadIdx.x] != 0.0) atomicAdd(B.moments + threadIdx.x, s_mom[threadIdx.x]);
-    for (int i = threadIdx.x; i < P.sbins; i += blockDim.x)
+    if (t < C_NUM && s_cnt[t]) atomicAdd(B.counters + t, s_cnt[t]);
+    if (t < 25 && s_mom[t] != 0.0) atomicAdd(B.moments + t, s_mom[t]);
+    for (int i = t; i < P.sbins; i += kBlock)
         if (s_bins[i]) atomicAdd(B.bins + i, (double)s_bins[i]);
 }
 
