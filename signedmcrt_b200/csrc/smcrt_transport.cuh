@@ -246,7 +246,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // The persistent kernel.  KERNEL: smcrt_kernel_kind.  REPLAY: injected streams.
 #ifndef SMCRT_MIN_BLOCKS
-#define SMCRT_MIN_BLOCKS 3
+#define SMCRT_MIN_BLOCKS 2
 #endif
 #ifndef SMCRT_WALK_SEGMENTS
 #define SMCRT_WALK_SEGMENTS 4
@@ -846,7 +846,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     __shared__ double s_mom[25];
     __shared__ int s_off[kGroups][Q][NW];
     __shared__ unsigned short s_list[kSlots];
-    __shared__ int s_total, s_stop;
+    __shared__ int s_stop;
     extern __shared__ __align__(16) unsigned char s_dyn[];
     Slots<R>& sl = *reinterpret_cast<Slots<R>*>(s_dyn);
     unsigned* s_bins = reinterpret_cast<unsigned*>(s_dyn + slots_bytes<R>());
@@ -880,12 +880,23 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
                 if (lane == 0) s_off[g][q][warp] = __popc(m);
             }
         }
+        if (t == 0) {
+            // device-side time budget: past it, stop and flag ABORTED
+            int stop = 0;
+            if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
+                atomicOr(B.status, STATUS_ABORTED);
+                stop = 1;
+            }
+            s_stop = stop;
+        }
         __syncthreads();
-        // exclusive scan over (group, q, warp): each group contiguous, slot order inside
-        if (warp == 0) {
+        // every warp scans the (group, q, warp) counts itself: each group is
+        // contiguous in the list, in slot order
+        int total;
+        {
             constexpr int E = kGroups * Q * NW;
             constexpr int PER = (E + 31) / 32;
-            int* flat = &s_off[0][0][0];
+            const int* flat = &s_off[0][0][0];
             int v[PER], sum = 0;
 #pragma unroll
             for (int k = 0; k < PER; ++k) {
@@ -899,32 +910,30 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
                 const int y = __shfl_up_sync(0xffffffffu, incl, d);
                 if ((int)lane >= d) incl += y;
             }
-            int run = incl - sum;
+            total = __shfl_sync(0xffffffffu, incl, 31);
+            const int excl = incl - sum;
 #pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                const int e = (int)lane * PER + k;
-                if (e < E) flat[e] = run;
-                run += v[k];
-            }
-            if (lane == 31) {
-                s_total = incl;
-                // device-side time budget: past it, stop and flag ABORTED
-                int stop = 0;
-                if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
-                    atomicOr(B.status, STATUS_ABORTED);
-                    stop = 1;
+            for (int q = 0; q < Q; ++q) {
+                // offset of entry (a[q], q, warp): held by lane e / PER as element e % PER
+                const int g = a[q] < kGroups ? a[q] : 0;
+                const int e = (g * Q + q) * NW + warp;
+                const int src = e / PER, k = e % PER;
+                int off = __shfl_sync(0xffffffffu, excl, src);
+#pragma unroll
+                for (int kk = 0; kk < PER; ++kk) {
+                    const int vk = __shfl_sync(0xffffffffu, v[kk], src);
+                    if (kk < k) off += vk;
                 }
-                s_stop = stop;
+                if (a[q] < kGroups) s_list[off + rank[q]] = (unsigned short)(t + q * kBlock);
             }
         }
+        const int stop = s_stop;
         __syncthreads();
-        const int total = s_total;
-        if (total == 0 || s_stop) break;
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-            if (a[q] < kGroups) s_list[s_off[a[q]][q][warp] + rank[q]] = (unsigned short)(t + q * kBlock);
-        __syncthreads();
-        // ---- one pass per listed packet
+        if (total == 0 || stop) break;
+        // ---- one pass per listed packet.  Warp w takes chunks w, w + 8, ... of
+        // the list, so the warps of a CTA work on different actions at a time
+        // (taking chunks in list order, all warps would run the same action and
+        // contend for the same pipes; measured slower).
         for (int i = t; i < total; i += kBlock) {
             const int s = s_list[i];
             int act = load_slot(sl, s, P, B, pk, f, rng);
