@@ -246,7 +246,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // The persistent kernel.  KERNEL: smcrt_kernel_kind.  REPLAY: injected streams.
 #ifndef SMCRT_MIN_BLOCKS
-#define SMCRT_MIN_BLOCKS 2
+#define SMCRT_MIN_BLOCKS 1
 #endif
 #ifndef SMCRT_WALK_SEGMENTS
 #define SMCRT_WALK_SEGMENTS 4
@@ -682,11 +682,20 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
 #ifndef SMCRT_SLOTS_PER_THREAD
 #define SMCRT_SLOTS_PER_THREAD 2
 #endif
-constexpr int kBlock = 256;
-constexpr int kSlots = kBlock * SMCRT_SLOTS_PER_THREAD;
+#ifndef SMCRT_BLOCK
+#define SMCRT_BLOCK 640
+#endif
+constexpr int kBlock = SMCRT_BLOCK;
+// Slots per thread: two for FP32 transport (132 bytes a slot); one for FP64
+// (172 bytes), so that a CTA's slots stay within the 227 KiB of shared memory.
+template <class R>
+struct SlotCount {
+    static constexpr int per_thread = sizeof(R) == 4 ? SMCRT_SLOTS_PER_THREAD : 1;
+    static constexpr int n = kBlock * per_thread;
+};
 constexpr int kGroups = 6;  // act values that are sorted (A_NEW .. A_DEATH)
 
-template <class R>
+template <class R, int kSlots = SlotCount<R>::n>
 struct Slots {
     static constexpr int kRW = sizeof(R) / 4;  // 32-bit words per R
     static constexpr int kUW = 4 * kRW + 3 > 8 ? 4 * kRW + 3 : 8;  // union words
@@ -702,7 +711,7 @@ struct Slots {
     uint32_t b0[kSlots], b1[kSlots], b2[kSlots], b3[kSlots];
 };
 
-template <class R>
+template <class R, int kSlots>
 __device__ __forceinline__ void put_r(uint32_t (*u)[kSlots], int k, int s, R v) {
     if (sizeof(R) == 4) {
         u[k][s] = __float_as_uint((float)v);
@@ -712,7 +721,7 @@ __device__ __forceinline__ void put_r(uint32_t (*u)[kSlots], int k, int s, R v) 
         u[k + 1][s] = (uint32_t)(b >> 32);
     }
 }
-template <class R>
+template <class R, int kSlots>
 __device__ __forceinline__ R get_r(const uint32_t (*u)[kSlots], int k, int s) {
     if (sizeof(R) == 4) return (R)__uint_as_float(u[k][s]);
     return (R)__longlong_as_double((long long)(((unsigned long long)u[k + 1][s] << 32) | u[k][s]));
@@ -830,7 +839,7 @@ __host__ __device__ constexpr size_t slots_bytes() {
 // The persistent, compacted kernel.  KERNEL: smcrt_kernel_kind.  REPLAY:
 // injected streams.
 //
-// A CTA holds kSlots packets in shared memory.  Each round it counting-sorts
+// A CTA holds SlotCount<R>::n packets in shared memory.  Each round it counting-sorts
 // its live slots by their next action (warp ballots, stable in slot order), then
 // every thread takes items t, t + kBlock, ... of the sorted list, runs one pass
 // of the packet's state machine and writes the packet back.  A warp therefore
@@ -840,12 +849,12 @@ __host__ __device__ constexpr size_t slots_bytes() {
 template <class R, int KERNEL, bool REPLAY>
 __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
                                                                              const Buffers B) {
-    constexpr int Q = SMCRT_SLOTS_PER_THREAD;
+    constexpr int Q = SlotCount<R>::per_thread;
     constexpr int NW = kBlock / 32;
     __shared__ unsigned long long s_cnt[C_NUM];
     __shared__ double s_mom[25];
     __shared__ int s_off[kGroups][Q][NW];
-    __shared__ unsigned short s_list[kSlots];
+    __shared__ unsigned short s_list[SlotCount<R>::n];
     __shared__ int s_stop;
     extern __shared__ __align__(16) unsigned char s_dyn[];
     Slots<R>& sl = *reinterpret_cast<Slots<R>*>(s_dyn);
