@@ -172,13 +172,113 @@ def run_reference(args, arr, st, workload: dict) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args) -> None:
+    """batch256: 256 instances of the box_slab geometry (64^3 grids) with per-instance
+    optics, packet counts (log-uniform 1e4..1e6) and seeds, in ONE graph-replayed
+    persistent launch; the same instances as 256 sequential plain launches are
+    timed beside it (same packets, so equal accuracy).  One GPU (replicas for N>1)."""
+    import torch
+    from signedmcrt_b200 import presets as P
+    from signedmcrt_b200.scene import FlatScene
+    from signedmcrt_b200.transport import Batch, Transport
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    st, optics, counts, seeds = P.batch_instances(scale=args.batch_scale)
+    ninst = len(counts)
+    total = int(counts.sum())
+    flat = FlatScene(P.box_slab())
+    workload = {"workload": f"batch256: {ninst} box_slab instances, mu_a~U(.01,1) mu_s~U(1,100) g~U(.7,.95) "
+                            f"n~U(1.33,1.45), packets round(10^U(4,6)) x {args.batch_scale}",
+                "grid": [64, 64, 64], "tally": "fp64", "instances": ninst, "packets_per_step": total}
+    if args.impl == "reference":
+        from oracle import binding as O
+        pol = O.reference_policy(tally_f32=True)
+        t_all, n_all = 0.0, 0
+        sub = max(1, int(round(1e-3 * total / 16)))
+        for i in range(0, ninst, 16):
+            arr = P.box_slab(mua=optics[i, 0, 1], mus=optics[i, 0, 0], g=optics[i, 0, 2], n=optics[i, 0, 3])
+            t = time.perf_counter()
+            O.run(arr, st, nphotons=sub, seed=int(seeds[i]), policy=pol)
+            t_all += time.perf_counter() - t
+            n_all += sub
+        v = n_all / t_all
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+                          "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f64", "data": "synthetic", "config": workload,
+                          "cpu_baseline": {"value": v, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
+                                           "sample": f"{sub} packets of every 16th instance"},
+                          "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    dev = torch.device("cuda", 0)
+    b = Batch(flat, st, ninst, optics=optics, precision=args.precision, timeout_ms=600000)
+    for w in range(args.warmup):
+        b.run(counts, seeds + 1000 * (w + 1), use_graph=True, want_jmean=False)
+    times, tot = [], None
+    with ClockSampler(0) as clk:
+        for k in range(args.steps):
+            _, _, _, tot = b.run(counts, seeds, use_graph=True, want_jmean=False)
+            times.append(tot["kernel_ms"])
+    ms = sum(times) / len(times)
+    value = total / (ms / 1e3)
+    # e2e: the same launch with the 512 MB of FP64 tallies copied to pinned host memory each step
+    host = torch.empty(ninst * b.ncell, dtype=torch.float64, pin_memory=True).numpy()
+    e_times = []
+    for k in range(args.steps):
+        t = time.perf_counter()
+        b.launch(counts, seeds, use_graph=True)
+        b.wait(jmean_out=host)
+        e_times.append(time.perf_counter() - t)
+    e_ms = 1e3 * sum(e_times) / len(e_times)
+    b.close()
+    # the same instances as sequential plain launches (one context each, one stream)
+    s = torch.cuda.Stream(dev)
+    trs = [Transport(P.box_slab(mua=o[0][1], mus=o[0][0], g=o[0][2], n=o[0][3]), st, precision=args.precision,
+                     stream=s.cuda_stream, timeout_ms=600000) for o in optics]
+    buf = torch.zeros(trs[0].ncell, dtype=torch.float64, device=dev)
+    for tr in trs:
+        tr.run_device(0, 1000, 1, buf.data_ptr(), None)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for tr, n, sd in zip(trs, counts, seeds):
+        tr.run_device(0, int(n), int(sd), buf.data_ptr(), None)
+    e1.record(s)
+    torch.cuda.synchronize(dev)
+    seq_ms = e0.elapsed_time(e1)
+    for tr in trs:
+        tr.close()
+    pk = peaks()
+    flop, nbytes = algorithmic_work(tot, flat)
+    fp32_peak = 148 * 128 * 2 * (pk["sm_max_mhz"] * 1e6) / 1e12
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+            "config": dict(workload, launch="one persistent kernel per step, replayed from a CUDA graph",
+                           l2="tallies 512 MB > L2"),
+            "sequential": {"value": total / (seq_ms / 1e3), "unit": UNIT, "ms_per_step": seq_ms,
+                           "launches": ninst, "speedup_of_batch": seq_ms / ms},
+            "roofline": {"bound": "hbm", "achieved": nbytes / (ms / 1e3) / 1e9, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": nbytes / (ms / 1e3) / 1e9 / pk["hbm_gbs"], "traffic": None,
+                         "peak_source": pk["source"],
+                         "fp32_issue": {"achieved_tflops": flop / (ms / 1e3) / 1e12, "peak_tflops": fp32_peak,
+                                        "frac": flop / (ms / 1e3) / 1e12 / fp32_peak}},
+            "gpu_launches": args.steps, "clocks": clk.summary(),
+            "e2e": {"value": total / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 16 * ninst + 8,
+                    "d2h_bytes_per_step": 8 * ninst * 64 ** 3, "ms_per_step": e_ms,
+                    "path": "smcrt_batch_launch + smcrt_batch_wait (C ABI, pinned host tallies)"}}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="sphere_water", choices=["sphere_water", "box_slab", "layered_vessels"])
+    ap.add_argument("--config", default="sphere_water",
+                    choices=["sphere_water", "box_slab", "layered_vessels", "batch256"])
+    ap.add_argument("--batch-scale", type=float, default=1.0, help="batch256: packet counts x this factor")
     ap.add_argument("--packets", type=float, default=0, help="packets per GPU per step (default: the config's)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample length")
@@ -191,6 +291,9 @@ def main() -> None:
 
     from signedmcrt_b200 import presets as P
     from signedmcrt_b200.scene import FlatScene
+    if args.config == "batch256":
+        run_batch(args)
+        return
     st = P.benchmark_settings(args.config)
     arr = P.setup_simulation(st)
     flat = FlatScene(arr)

@@ -255,9 +255,51 @@ int32_t smcrt_replay(smcrt_ctx* ctx, const double* uniforms, const int64_t* offs
                      int64_t npackets, double* jmean, double* det_bins,
                      smcrt_packet_state* states, smcrt_stats* stats);
 
-/* Batched: ninst independent contexts (same precision/kernel) run in ONE
- * persistent launch with uneven packet counts.  jmeans[i]/bins[i] are host
- * buffers (or NULL). */
+/* ---- batches ----------------------------------------------------------------
+ * Many instances of one scene -- the same geometry, grid, source, detectors and
+ * options, each with its own region optics, packet count and seed -- transported
+ * in ONE persistent launch (pathlength and weight kernels).  Instance i runs
+ * packets [0, nphotons[i]) of stream seeds[i]: the packets smcrt_run would run
+ * with that seed and those optics, so a batch equals its instances run one by one
+ * (FP64: identical event counts).  No counterpart in the reference, which runs one
+ * simulation per process. */
+typedef struct smcrt_region_optics {
+    double mus, mua, hgg, n;  /* as in smcrt_region */
+} smcrt_region_optics;
+typedef struct smcrt_batch smcrt_batch;
+
+/* Creates a batch of ninst instances (1..262143), all with the scene's optics;
+ * allocates the instances' FP64 tallies (ninst*ncell, instance-major) and
+ * detector bins (ninst*nbins) on the device. */
+int32_t smcrt_batch_create(const smcrt_scene* scene, const smcrt_grid* grid,
+                           const smcrt_source* source, const smcrt_detector* dets,
+                           int32_t ndet, const smcrt_options* opts, int32_t ninst,
+                           smcrt_batch** out);
+/* Sets every instance's region optics: optics[i*nregions + r] for instance i,
+ * region r (scene order).  Waits for a launch in flight. */
+int32_t smcrt_batch_set_optics(smcrt_batch* b, const smcrt_region_optics* optics);
+/* Zeroes the batch tallies and launches all instances asynchronously on the
+ * batch's stream.  use_graph != 0: the table upload, the zeroing and the kernel are
+ * captured into a CUDA graph on the first such call and replayed after that
+ * (packet counts and seeds are device data and may change between calls). */
+int32_t smcrt_batch_launch(smcrt_batch* b, const int64_t* nphotons, const uint64_t* seeds,
+                           int32_t use_graph);
+/* Waits for the launch (bounded by the time limit) and copies to HOST buffers
+ * (each may be NULL): jmean (ninst*ncell), det_bins (ninst*nbins),
+ * per_instance[i] (packets, rng_draws and nscatt of instance i) and total (the
+ * event counters of the whole launch). */
+int32_t smcrt_batch_wait(smcrt_batch* b, double* jmean, double* det_bins,
+                         smcrt_stats* per_instance, smcrt_stats* total);
+/* Device addresses of the batch tallies (valid until smcrt_batch_destroy). */
+int32_t smcrt_batch_device_tallies(smcrt_batch* b, double** jmean_dev, double** det_bins_dev);
+/* The batch's cudaStream_t, for ordering caller work after a launch. */
+int64_t smcrt_batch_stream(const smcrt_batch* b);
+void smcrt_batch_destroy(smcrt_batch* b);
+
+/* Batched run over contexts: ninst contexts whose scenes share their geometry
+ * (region optics may differ) run as one batch launch; jmeans[i] / det_bins[i] are
+ * host buffers (or NULL), stats[i] gets packets, rng_draws and nscatt.  Contexts
+ * with different geometry, or test kernels, run one launch each. */
 int32_t smcrt_run_batched(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* nphotons,
                           const uint64_t* seeds, double* const* jmeans,
                           double* const* det_bins, smcrt_stats* stats);

@@ -119,6 +119,10 @@ def i32ptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
 
 
+class RegionOptics(C.Structure):
+    _fields_ = [("mus", C.c_double), ("mua", C.c_double), ("hgg", C.c_double), ("n", C.c_double)]
+
+
 # Exported symbols of include/smcrt.h with their argtypes/restype.
 SIGNATURES = {
     "smcrt_abi_version": ([], C.c_int32),
@@ -136,6 +140,15 @@ SIGNATURES = {
     "smcrt_run_batched": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_uint64),
                            C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_double)), C.POINTER(Stats)],
                           C.c_int32),
+    "smcrt_batch_create": ([C.POINTER(Scene), C.POINTER(Grid), C.POINTER(Source), C.POINTER(Detector), C.c_int32,
+                            C.POINTER(Options), C.c_int32, C.POINTER(C.c_void_p)], C.c_int32),
+    "smcrt_batch_set_optics": ([C.c_void_p, C.POINTER(RegionOptics)], C.c_int32),
+    "smcrt_batch_launch": ([C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), C.c_int32], C.c_int32),
+    "smcrt_batch_wait": ([C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(Stats),
+                          C.POINTER(Stats)], C.c_int32),
+    "smcrt_batch_device_tallies": ([C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)], C.c_int32),
+    "smcrt_batch_stream": ([C.c_void_p], C.c_int64),
+    "smcrt_batch_destroy": ([C.c_void_p], None),
     "smcrt_run_device_static": ([C.POINTER(Scene), C.POINTER(Grid), C.POINTER(Source), C.POINTER(Detector),
                                  C.c_int32, C.POINTER(Options), C.c_int64, C.c_int64, C.c_uint64, C.c_void_p,
                                  C.c_void_p, C.POINTER(Stats)], C.c_int32),

@@ -640,10 +640,505 @@ int32_t smcrt_replay(smcrt_ctx* c, const double* uniforms, const int64_t* offset
     return read_stats(c, stats);
 }
 
+}  // extern "C"
+
+// ===========================================================================
+// Batches: instances of one scene geometry, each with its own region optics,
+// packet count and seed, transported in ONE persistent launch.  The kernel maps
+// a launch packet id to (instance, instance packet id) through a prefix table
+// in device memory, so packet counts and seeds are data: a captured CUDA graph
+// stays valid when they change.
+struct smcrt_batch {
+    int device = 0, nsm = 0, precision = SMCRT_FP32, kernel = SMCRT_KERNEL_PATHLENGTH;
+    int ninst = 0, grid_blocks = 0, timeout_ms = 600000;
+    long long ncell = 0, nbins = 0;
+    cudaStream_t stream = nullptr;
+    Params<float>* pf = nullptr;
+    Params<double>* pd = nullptr;
+    std::vector<smcrt_region> regions;  // the base scene, for smcrt_batch_set_optics
+    std::vector<smcrt_prim> prims;
+    double* d_jm = nullptr;
+    double* d_bins = nullptr;
+    void* d_opt = nullptr;
+    long long* d_prefix = nullptr;
+    unsigned long long* d_seed = nullptr;
+    unsigned long long* d_bstats = nullptr;
+    unsigned long long* d_work = nullptr;  // [0] work, [1..C_NUM] counters
+    double* d_mom = nullptr;
+    int* d_status = nullptr;
+    long long* h_prefix = nullptr;          // pinned staging of the tables
+    unsigned long long* h_seed = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool pending = false;
+};
+
+namespace {
+
+template <class R>
+void optics_of(const SceneT<R>& sc, const SceneT<double>& sc64, InstOptics<R>& o) {
+    std::memset(&o, 0, sizeof(o));
+    for (int r = 0; r < sc.nregions; ++r) {
+        o.kappa[r] = sc.region[r].kappa;
+        o.albedo[r] = sc.region[r].albedo;
+        o.hgg[r] = sc.region[r].hgg;
+        o.g2[r] = sc.region[r].g2;
+        o.nidx[r] = sc.region[r].nidx;
+        o.nidx64[r] = sc64.region[r].nidx;
+    }
+}
+
+template <class R>
+Params<R>* batch_params(smcrt_batch* b);
+template <>
+Params<float>* batch_params<float>(smcrt_batch* b) { return b->pf; }
+template <>
+Params<double>* batch_params<double>(smcrt_batch* b) { return b->pd; }
+
+// Device buffers and tables of a batch whose parameters (b->pf or b->pd) are set.
+template <class R>
+int batch_alloc(smcrt_batch* b) {
+    CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&b->d_jm, sizeof(double) * (size_t)b->ninst * (size_t)b->ncell));
+    CK(cudaMalloc(&b->d_bins, sizeof(double) * (size_t)std::max(1ll, b->ninst * b->nbins)));
+    CK(cudaMalloc(&b->d_opt, sizeof(InstOptics<R>) * (size_t)b->ninst));
+    CK(cudaMalloc(&b->d_prefix, sizeof(long long) * (size_t)(b->ninst + 1)));
+    CK(cudaMalloc(&b->d_seed, sizeof(unsigned long long) * (size_t)b->ninst));
+    CK(cudaMalloc(&b->d_bstats, sizeof(unsigned long long) * 3 * (size_t)b->ninst));
+    CK(cudaMalloc(&b->d_work, sizeof(unsigned long long) * (1 + C_NUM)));
+    CK(cudaMalloc(&b->d_mom, sizeof(double) * 25));
+    CK(cudaMalloc(&b->d_status, sizeof(int)));
+    CK(cudaMallocHost(&b->h_prefix, sizeof(long long) * (size_t)(b->ninst + 1)));
+    CK(cudaMallocHost(&b->h_seed, sizeof(unsigned long long) * (size_t)b->ninst));
+    CK(cudaEventCreate(&b->ev0));
+    CK(cudaEventCreate(&b->ev1));
+    Params<R>* P = batch_params<R>(b);
+    P->bopt = (const InstOptics<R>*)b->d_opt;
+    P->bprefix = b->d_prefix;
+    P->bseed = b->d_seed;
+    P->bstats = b->d_bstats;
+    P->ninst = b->ninst;
+    P->nbins = b->nbins;
+    P->sbins = 0;
+    P->tcopies = 1;
+    P->tmask = 0;
+    P->ncell = b->ncell;
+    for (int k = 0; k < kMaxTallyCopies; ++k) P->jtab[k] = k == 0 ? b->d_jm : nullptr;
+    P->first = 0;
+    P->count = 0;
+    int per_sm = 0;
+    int rc = resident_per_sm(b->precision, b->kernel, kBlock, 0, 0, &per_sm);
+    if (rc) return rc;
+    b->grid_blocks = b->nsm * per_sm;
+    // set the kernel's shared-memory limit now, outside any stream capture
+    cudaError_t e = b->precision == SMCRT_FP64
+                        ? (b->kernel == SMCRT_KERNEL_WEIGHT ? launch_batch_f64_1(*b->pd, Buffers{}, 0, b->stream)
+                                                            : launch_batch_f64_0(*b->pd, Buffers{}, 0, b->stream))
+                        : (b->kernel == SMCRT_KERNEL_WEIGHT ? launch_batch_f32_1(*b->pf, Buffers{}, 0, b->stream)
+                                                            : launch_batch_f32_0(*b->pf, Buffers{}, 0, b->stream));
+    if (e != cudaSuccess && e != cudaErrorInvalidConfiguration)
+        return fail(SMCRT_ERR_CUDA, std::string("batch kernel set-up: ") + cudaGetErrorString(e));
+    cudaGetLastError();
+    return SMCRT_OK;
+}
+
+template <class R>
+int batch_upload_optics(smcrt_batch* b, const std::vector<InstOptics<R>>& o) {
+    CK(cudaMemcpyAsync(b->d_opt, o.data(), sizeof(InstOptics<R>) * o.size(), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    return SMCRT_OK;
+}
+
+// The launch sequence: tables in, tallies and counters zeroed, the kernel.
+int batch_enqueue(smcrt_batch* b) {
+    cudaStream_t s = b->stream;
+    CK(cudaMemcpyAsync(b->d_prefix, b->h_prefix, sizeof(long long) * (size_t)(b->ninst + 1), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(b->d_seed, b->h_seed, sizeof(unsigned long long) * (size_t)b->ninst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(b->d_jm, 0, sizeof(double) * (size_t)b->ninst * (size_t)b->ncell, s));
+    CK(cudaMemsetAsync(b->d_bins, 0, sizeof(double) * (size_t)std::max(1ll, b->ninst * b->nbins), s));
+    CK(cudaMemsetAsync(b->d_bstats, 0, sizeof(unsigned long long) * 3 * (size_t)b->ninst, s));
+    CK(cudaMemsetAsync(b->d_work, 0, sizeof(unsigned long long) * (1 + C_NUM), s));
+    CK(cudaMemsetAsync(b->d_mom, 0, sizeof(double) * 25, s));
+    CK(cudaMemsetAsync(b->d_status, 0, sizeof(int), s));
+    Buffers B{};
+    B.jmean = b->d_jm;
+    B.bins = b->d_bins;
+    B.work = b->d_work;
+    B.counters = b->d_work + 1;
+    B.moments = b->d_mom;
+    B.status = b->d_status;
+    cudaError_t e;
+    if (b->precision == SMCRT_FP64)
+        e = b->kernel == SMCRT_KERNEL_WEIGHT ? launch_batch_f64_1(*b->pd, B, b->grid_blocks, s)
+                                             : launch_batch_f64_0(*b->pd, B, b->grid_blocks, s);
+    else
+        e = b->kernel == SMCRT_KERNEL_WEIGHT ? launch_batch_f32_1(*b->pf, B, b->grid_blocks, s)
+                                             : launch_batch_f32_0(*b->pf, B, b->grid_blocks, s);
+    if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    return SMCRT_OK;
+}
+
+int batch_wait(smcrt_batch* b) {
+    auto t0 = std::chrono::steady_clock::now();
+    const double limit = (double)b->timeout_ms + 30000.0;
+    for (;;) {
+        cudaError_t e = cudaEventQuery(b->ev1);
+        if (e == cudaSuccess) return SMCRT_OK;
+        if (e != cudaErrorNotReady) return fail(SMCRT_ERR_CUDA, std::string("batch kernel: ") + cudaGetErrorString(e));
+        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > limit) return fail(SMCRT_ERR_TIMEOUT, "batch kernel did not finish within its time limit");
+        std::this_thread::sleep_for(std::chrono::microseconds(ms < 10 ? 20 : 500));
+    }
+}
+
+void batch_free(smcrt_batch* b) {
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->d_jm);
+    cudaFree(b->d_bins);
+    cudaFree(b->d_opt);
+    cudaFree(b->d_prefix);
+    cudaFree(b->d_seed);
+    cudaFree(b->d_bstats);
+    cudaFree(b->d_work);
+    cudaFree(b->d_mom);
+    cudaFree(b->d_status);
+    if (b->h_prefix) cudaFreeHost(b->h_prefix);
+    if (b->h_seed) cudaFreeHost(b->h_seed);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b->pf;
+    delete b->pd;
+    delete b;
+}
+
+// Per-instance optics of a batch from `ninst` scenes that differ from the base
+// scene only in their region optics (converted as smcrt_create converts them).
+template <class R>
+int batch_optics_from_regions(smcrt_batch* b, const smcrt_region_optics* optics) {
+    const int nr = (int)b->regions.size();
+    std::vector<InstOptics<R>> o((size_t)b->ninst);
+    std::vector<smcrt_region> regs(b->regions);
+    smcrt_scene sc{nr, (int32_t)b->prims.size(), regs.data(), b->prims.data()};
+    SceneT<R>* s1 = new SceneT<R>;
+    SceneT<double>* s2 = new SceneT<double>;
+    for (int i = 0; i < b->ninst; ++i) {
+        for (int r = 0; r < nr; ++r) {
+            if (optics) {
+                const smcrt_region_optics& q = optics[(size_t)i * nr + r];
+                regs[r].mus = q.mus;
+                regs[r].mua = q.mua;
+                regs[r].hgg = q.hgg;
+                regs[r].n = q.n;
+            }
+        }
+        int rc = validate_optics(&sc);
+        if (rc) {
+            delete s1;
+            delete s2;
+            return fail(rc, "batch instance " + std::to_string(i) + ": " + g_err);
+        }
+        fill_scene(*s1, &sc);
+        fill_scene(*s2, &sc);
+        optics_of(*s1, *s2, o[(size_t)i]);
+    }
+    delete s1;
+    delete s2;
+    return batch_upload_optics<R>(b, o);
+}
+
+int batch_set_counts(smcrt_batch* b, const int64_t* nphotons, const uint64_t* seeds) {
+    if (!nphotons || !seeds) return fail(SMCRT_ERR_ARG, "batch: nphotons and seeds are required");
+    long long acc = 0;
+    b->h_prefix[0] = 0;
+    for (int i = 0; i < b->ninst; ++i) {
+        if (nphotons[i] < 0) return fail(SMCRT_ERR_ARG, "batch: negative packet count");
+        acc += nphotons[i];
+        b->h_prefix[i + 1] = acc;
+        b->h_seed[i] = seeds[i];
+    }
+    return SMCRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t smcrt_batch_create(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* source,
+                           const smcrt_detector* dets, int32_t ndet, const smcrt_options* opts, int32_t ninst,
+                           smcrt_batch** out) {
+    g_err.clear();
+    if (!out) return fail(SMCRT_ERR_ARG, "out is null");
+    *out = nullptr;
+    if (ninst < 1 || ninst > (1 << 18) - 1) return fail(SMCRT_ERR_ARG, "batch: ninst must be 1..262143");
+    int rc = validate_scene(scene);
+    if (rc) return rc;
+    rc = validate_optics(scene);
+    if (rc) return rc;
+    if (!grid || grid->nxg <= 0 || grid->nyg <= 0 || grid->nzg <= 0 || !(grid->xmax > 0) || !(grid->ymax > 0) ||
+        !(grid->zmax > 0))
+        return fail(SMCRT_ERR_ARG, "grid: need positive voxel counts and half sizes");
+    if (!source || source->kind < SMCRT_SRC_POINT || source->kind > SMCRT_SRC_FOCUS)
+        return fail(SMCRT_ERR_ARG, "source: unknown kind");
+    if (ndet < 0 || ndet > kMaxDetectors || (ndet > 0 && !dets))
+        return fail(SMCRT_ERR_ARG, "detectors: 0.." + std::to_string(kMaxDetectors) + " supported");
+    const int prec = opts ? opts->precision : SMCRT_FP32;
+    const int kern = opts ? opts->kernel : SMCRT_KERNEL_PATHLENGTH;
+    if (prec != SMCRT_FP32 && prec != SMCRT_FP64) return fail(SMCRT_ERR_ARG, "options: unknown precision");
+    if (kern != SMCRT_KERNEL_PATHLENGTH && kern != SMCRT_KERNEL_WEIGHT)
+        return fail(SMCRT_ERR_ARG, "batch: pathlength and weight kernels only");
+    if (opts && opts->block_size > 0 && opts->block_size != kBlock)
+        return fail(SMCRT_ERR_ARG, "options: block_size must be 0 or " + std::to_string(kBlock));
+    DetT dtab[kMaxDetectors];
+    long long nbins = 0;
+    rc = fill_dets(dtab, dets, ndet, scene->nregions, nbins);
+    if (rc) return rc;
+    smcrt_batch* b = new smcrt_batch;
+    rc = pick_device(b->device, b->nsm);
+    if (rc) {
+        delete b;
+        return rc;
+    }
+    b->precision = prec;
+    b->kernel = kern;
+    b->ninst = ninst;
+    b->ncell = (long long)grid->nxg * grid->nyg * grid->nzg;
+    b->nbins = nbins;
+    b->timeout_ms = (opts && opts->timeout_ms > 0) ? opts->timeout_ms : 600000;
+    b->regions.assign(scene->regions, scene->regions + scene->nregions);
+    b->prims.assign(scene->prims, scene->prims + scene->nprims);
+    if (prec == SMCRT_FP64) b->pd = make_params<double>(scene, grid, source, dtab, ndet, opts);
+    else b->pf = make_params<float>(scene, grid, source, dtab, ndet, opts);
+    rc = prec == SMCRT_FP64 ? batch_alloc<double>(b) : batch_alloc<float>(b);
+    if (!rc) rc = prec == SMCRT_FP64 ? batch_optics_from_regions<double>(b, nullptr)
+                                     : batch_optics_from_regions<float>(b, nullptr);
+    if (rc) {
+        batch_free(b);
+        return rc;
+    }
+    *out = b;
+    return SMCRT_OK;
+}
+
+int32_t smcrt_batch_set_optics(smcrt_batch* b, const smcrt_region_optics* optics) {
+    g_err.clear();
+    if (!b || !optics) return fail(SMCRT_ERR_ARG, "batch_set_optics: null argument");
+    if (b->pending) {
+        int rc = batch_wait(b);
+        if (rc) return rc;
+    }
+    return b->precision == SMCRT_FP64 ? batch_optics_from_regions<double>(b, optics)
+                                      : batch_optics_from_regions<float>(b, optics);
+}
+
+int32_t smcrt_batch_launch(smcrt_batch* b, const int64_t* nphotons, const uint64_t* seeds, int32_t use_graph) {
+    g_err.clear();
+    if (!b) return fail(SMCRT_ERR_ARG, "batch is null");
+    if (b->pending) {  // the staging buffers feed the previous launch until it ends
+        int rc = batch_wait(b);
+        if (rc) return rc;
+    }
+    int rc = batch_set_counts(b, nphotons, seeds);
+    if (rc) return rc;
+    CK(cudaEventRecord(b->ev0, b->stream));
+    if (use_graph) {
+        if (!b->exec) {
+            CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            rc = batch_enqueue(b);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+            b->graph = g;
+            CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        }
+        CK(cudaGraphLaunch(b->exec, b->stream));
+    } else {
+        rc = batch_enqueue(b);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(b->ev1, b->stream));
+    b->pending = true;
+    return SMCRT_OK;
+}
+
+int32_t smcrt_batch_wait(smcrt_batch* b, double* jmean, double* det_bins, smcrt_stats* per_instance,
+                         smcrt_stats* total) {
+    g_err.clear();
+    if (!b) return fail(SMCRT_ERR_ARG, "batch is null");
+    if (!b->pending) return fail(SMCRT_ERR_ARG, "batch_wait: nothing launched");
+    int rc = batch_wait(b);
+    if (rc) return rc;
+    b->pending = false;
+    if (jmean)
+        CK(cudaMemcpy(jmean, b->d_jm, sizeof(double) * (size_t)b->ninst * (size_t)b->ncell, cudaMemcpyDeviceToHost));
+    if (det_bins && b->nbins > 0)
+        CK(cudaMemcpy(det_bins, b->d_bins, sizeof(double) * (size_t)b->ninst * (size_t)b->nbins,
+                      cudaMemcpyDeviceToHost));
+    unsigned long long cnt[1 + C_NUM];
+    double mom[25];
+    int status = 0;
+    CK(cudaMemcpy(cnt, b->d_work, sizeof(cnt), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(mom, b->d_mom, sizeof(mom), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&status, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    if (per_instance) {
+        std::vector<unsigned long long> bs(3 * (size_t)b->ninst);
+        CK(cudaMemcpy(bs.data(), b->d_bstats, sizeof(unsigned long long) * bs.size(), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < b->ninst; ++i) {
+            smcrt_stats& st = per_instance[i];
+            std::memset(&st, 0, sizeof(st));
+            st.packets = bs[3 * (size_t)i];
+            st.rng_draws = bs[3 * (size_t)i + 1];
+            st.nscatt = (double)bs[3 * (size_t)i + 2];
+            st.kernel_ms = ms;
+            st.device_status = status;
+        }
+    }
+    if (total) {
+        std::memset(total, 0, sizeof(*total));
+        const unsigned long long* k = cnt + 1;
+        total->packets = k[C_PACKETS];
+        total->sdf_evals = k[C_SDF];
+        total->voxel_segments = k[C_VOX];
+        total->trace_steps = k[C_STEPS];
+        total->scatters = k[C_SCAT];
+        total->fresnel_events = k[C_FRES];
+        total->reflections = k[C_REFL];
+        total->kills_step_cap = k[C_STEPCAP];
+        total->kills_error = k[C_ERR];
+        total->rng_draws = k[C_DRAWS];
+        total->nscatt = mom[24];
+        total->kernel_ms = ms;
+        total->device_status = status;
+    }
+    if (status & STATUS_ABORTED) return fail(SMCRT_ERR_TIMEOUT, "batch kernel reached its time limit and stopped early");
+    if (status & (STATUS_STREAM_EXHAUSTED | STATUS_BAD_INDEX))
+        return fail(SMCRT_ERR_DEVICE, "device status flag " + std::to_string(status));
+    return SMCRT_OK;
+}
+
+int32_t smcrt_batch_device_tallies(smcrt_batch* b, double** jmean_dev, double** det_bins_dev) {
+    g_err.clear();
+    if (!b) return fail(SMCRT_ERR_ARG, "batch is null");
+    if (jmean_dev) *jmean_dev = b->d_jm;
+    if (det_bins_dev) *det_bins_dev = b->d_bins;
+    return SMCRT_OK;
+}
+
+int64_t smcrt_batch_stream(const smcrt_batch* b) { return b ? (int64_t)(intptr_t)b->stream : 0; }
+
+void smcrt_batch_destroy(smcrt_batch* b) {
+    if (b) batch_free(b);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The scene geometry, grid, source, detectors and run options of two contexts'
+// parameter blocks are equal (region optics may differ).
+template <class R>
+bool same_geometry(const Params<R>& a, const Params<R>& b) {
+    if (a.sc.nregions != b.sc.nregions || a.sc.nprims != b.sc.nprims) return false;
+    if (std::memcmp(a.sc.prim, b.sc.prim, sizeof(a.sc.prim[0]) * (size_t)a.sc.nprims)) return false;
+    for (int r = 0; r < a.sc.nregions; ++r) {
+        const DRegion<R>&x = a.sc.region[r], &y = b.sc.region[r];
+        if (x.first != y.first || x.n != y.n || x.op != y.op || x.k != y.k) return false;
+    }
+    return !std::memcmp(&a.grid, &b.grid, sizeof(a.grid)) && !std::memcmp(&a.src, &b.src, sizeof(a.src)) &&
+           a.ndet == b.ndet && !std::memcmp(a.det, b.det, sizeof(a.det[0]) * (size_t)a.ndet) &&
+           a.kernel == b.kernel && a.end_early == b.end_early && a.max_steps == b.max_steps && a.eps == b.eps &&
+           a.normal_h == b.normal_h && a.instance == b.instance;
+}
+
+template <class R>
+const Params<R>* ctx_params(const smcrt_ctx* c);
+template <>
+const Params<float>* ctx_params<float>(const smcrt_ctx* c) { return c->pf; }
+template <>
+const Params<double>* ctx_params<double>(const smcrt_ctx* c) { return c->pd; }
+
+// One batch launch over contexts that share their geometry; done = false when
+// they do not (the caller then runs them one by one).
+template <class R>
+int run_batched_t(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* nphotons, const uint64_t* seeds,
+                  double* const* jmeans, double* const* det_bins, smcrt_stats* stats, bool& done) {
+    done = false;
+    const Params<R>* P0 = ctx_params<R>(ctxs[0]);
+    if (ctxs[0]->kernel == SMCRT_KERNEL_TEST) return SMCRT_OK;
+    for (int i = 1; i < ninst; ++i)
+        if (ctxs[i]->precision != ctxs[0]->precision || ctxs[i]->device != ctxs[0]->device ||
+            !same_geometry(*P0, *ctx_params<R>(ctxs[i])))
+            return SMCRT_OK;
+    smcrt_batch* b = new smcrt_batch;
+    b->device = ctxs[0]->device;
+    b->nsm = ctxs[0]->nsm;
+    b->precision = ctxs[0]->precision;
+    b->kernel = ctxs[0]->kernel;
+    b->ninst = ninst;
+    b->ncell = ctxs[0]->ncell;
+    b->nbins = ctxs[0]->nbins;
+    b->timeout_ms = ctxs[0]->timeout_ms;
+    if (sizeof(R) == 8) b->pd = new Params<double>(*ctxs[0]->pd);
+    else b->pf = new Params<float>(*ctxs[0]->pf);
+    int rc = batch_alloc<R>(b);
+    if (!rc) {
+        std::vector<InstOptics<R>> o((size_t)ninst);
+        for (int i = 0; i < ninst; ++i) {
+            const Params<R>* Pi = ctx_params<R>(ctxs[i]);
+            optics_of(Pi->sc, Pi->sc64, o[(size_t)i]);
+        }
+        rc = batch_upload_optics<R>(b, o);
+    }
+    if (!rc) rc = smcrt_batch_launch(b, nphotons, seeds, 0);
+    std::vector<smcrt_stats> per((size_t)ninst);
+    if (!rc) rc = smcrt_batch_wait(b, nullptr, nullptr, per.data(), nullptr);
+    for (int i = 0; !rc && i < ninst; ++i) {
+        if (jmeans && jmeans[i])
+            if (cudaMemcpy(jmeans[i], b->d_jm + (size_t)i * b->ncell, sizeof(double) * (size_t)b->ncell,
+                           cudaMemcpyDeviceToHost) != cudaSuccess)
+                rc = fail(SMCRT_ERR_CUDA, "batched: tally copy failed");
+        if (!rc && det_bins && det_bins[i] && b->nbins > 0)
+            if (cudaMemcpy(det_bins[i], b->d_bins + (size_t)i * b->nbins, sizeof(double) * (size_t)b->nbins,
+                           cudaMemcpyDeviceToHost) != cudaSuccess)
+                rc = fail(SMCRT_ERR_CUDA, "batched: bin copy failed");
+        if (stats) stats[i] = per[(size_t)i];
+    }
+    batch_free(b);
+    done = rc == SMCRT_OK;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
 int32_t smcrt_run_batched(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* nphotons, const uint64_t* seeds,
                           double* const* jmeans, double* const* det_bins, smcrt_stats* stats) {
     g_err.clear();
-    return fail(SMCRT_ERR_ARG, "smcrt_run_batched: not available in this build");
+    if (!ctxs || ninst < 1 || !nphotons || !seeds) return fail(SMCRT_ERR_ARG, "run_batched: bad arguments");
+    for (int i = 0; i < ninst; ++i)
+        if (!ctxs[i]) return fail(SMCRT_ERR_ARG, "run_batched: null context");
+    bool done = false;
+    int rc = ctxs[0]->precision == SMCRT_FP64
+                 ? run_batched_t<double>(ctxs, ninst, nphotons, seeds, jmeans, det_bins, stats, done)
+                 : run_batched_t<float>(ctxs, ninst, nphotons, seeds, jmeans, det_bins, stats, done);
+    if (rc || done) return rc;
+    // contexts with different geometry (or test kernels): one launch each
+    for (int i = 0; i < ninst; ++i) {
+        rc = smcrt_run(ctxs[i], nphotons[i], seeds[i], jmeans ? jmeans[i] : nullptr,
+                       det_bins ? det_bins[i] : nullptr, stats ? &stats[i] : nullptr);
+        if (rc) return rc;
+    }
+    return SMCRT_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -57,6 +57,14 @@ struct DRegion {
     R k, kappa, albedo, hgg, g2, nidx;
 };
 
+// Optical properties of one batch instance, per region (the per-region fields of
+// DRegion; the geometry is shared by all instances of a batch).
+template <class R>
+struct InstOptics {
+    R kappa[kMaxRegions], albedo[kMaxRegions], hgg[kMaxRegions], g2[kMaxRegions], nidx[kMaxRegions];
+    double nidx64[kMaxRegions];
+};
+
 template <class R>
 struct SceneT {
     int nregions, nprims;
@@ -445,6 +453,15 @@ struct Params {
     unsigned tmask;                  // tcopies - 1 (tcopies is a power of two)
     long long ncell;
     double* jtab[kMaxTallyCopies];   // the grid of each copy; jtab[0] is the output grid
+    // batch launches: instance i has packets [bprefix[i], bprefix[i+1]) of the
+    // launch, seed bseed[i], optics bopt[i], tally jtab[0] + i * ncell and
+    // detector bins + i * nbins; per-instance packets/draws/scatters in bstats
+    const InstOptics<R>* bopt;
+    const long long* bprefix;
+    const unsigned long long* bseed;
+    unsigned long long* bstats;  // [ninst][3]
+    int ninst;
+    long long nbins;
 };
 
 }  // namespace smcrt

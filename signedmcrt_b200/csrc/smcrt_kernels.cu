@@ -34,6 +34,23 @@ cudaError_t SMCRT_CAT(launch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, cons
     return cudaGetLastError();
 }
 
+// Batch launches (pathlength and weight kernels): instances sharing the scene
+// geometry; the per-instance tables are in device memory behind P.
+cudaError_t SMCRT_CAT(launch_batch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, const Buffers& B, int blocks,
+                                                         cudaStream_t s) {
+#if SMCRT_K == 2
+    (void)P; (void)B; (void)blocks; (void)s;
+    return cudaErrorNotSupported;
+#else
+    static const cudaError_t attr = cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, false, true>,
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         (int)slots_bytes<SMCRT_R>());
+    if (attr != cudaSuccess) return attr;
+    transport_kernel<SMCRT_R, SMCRT_K, false, true><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
+    return cudaGetLastError();
+#endif
+}
+
 cudaError_t SMCRT_CAT(occupancy, SMCRT_TAG, SMCRT_K)(int block, size_t sbins_bytes, int* per_sm) {
     if (block != kBlock) return cudaErrorInvalidConfiguration;
     cudaError_t e = allow_smem<false>();

@@ -10,7 +10,8 @@ namespace smcrt {
 #define SMCRT_DECL_VARIANT(R, TAG, K)                                                                       \
     cudaError_t launch_##TAG##_##K(const Params<R>& P, const Buffers& B, bool replay, int blocks, int block, \
                                    cudaStream_t s);                                                       \
-    cudaError_t occupancy_##TAG##_##K(int block, size_t sbins_bytes, int* per_sm);
+    cudaError_t occupancy_##TAG##_##K(int block, size_t sbins_bytes, int* per_sm);                   \
+    cudaError_t launch_batch_##TAG##_##K(const Params<R>& P, const Buffers& B, int blocks, cudaStream_t s);
 
 SMCRT_DECL_VARIANT(float, f32, 0)
 SMCRT_DECL_VARIANT(float, f32, 1)

@@ -54,6 +54,7 @@ struct Pk {
     int bounces;
     int nscatt;
     int flags;
+    int inst;  // batch instance (0 outside batches)
     bool tflag;
 };
 
@@ -229,11 +230,26 @@ __device__ __forceinline__ void record_detectors(const Params<R>& P, double* bin
 // The fluence grid this CTA adds into: copy (CTA index mod tcopies).  The CTA
 // index is read at each use (volatile) rather than kept in a register across the
 // transport loop, and the copy's address comes from the parameter bank.
-template <class R>
-__device__ __forceinline__ double* tally_grid(const Params<R>& P) {
+template <class R, bool BATCH>
+__device__ __forceinline__ double* tally_grid(const Params<R>& P, int inst) {
+    if (BATCH) return P.jtab[0] + (long long)inst * P.ncell;  // one grid per instance, no copies
     unsigned b;
     asm volatile("mov.u32 %0, %%ctaid.x;" : "=r"(b));
     return P.jtab[b & P.tmask];
+}
+
+// Region optics: the scene's, or the batch instance's.
+template <class R, bool BATCH>
+__device__ __forceinline__ R opt_kappa(const Params<R>& P, int inst, int r) {
+    return BATCH ? P.bopt[inst].kappa[r] : P.sc.region[r].kappa;
+}
+template <class R, bool BATCH>
+__device__ __forceinline__ R opt_nidx(const Params<R>& P, int inst, int r) {
+    return BATCH ? P.bopt[inst].nidx[r] : P.sc.region[r].nidx;
+}
+template <class R, bool BATCH>
+__device__ __forceinline__ double opt_nidx64(const Params<R>& P, int inst, int r) {
+    return BATCH ? P.bopt[inst].nidx64[r] : P.sc64.region[r].nidx;
 }
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -299,10 +315,10 @@ __device__ __forceinline__ V3<R> grid_origin(const GridT<R>& g, const V3<double>
 // Starts a sphere-tracing step of length f.dsdf (body of the while loop at
 // inttau2.f90:63-83): optical depth bookkeeping, then the voxel-walk setup.
 // Returns A_WALK, or -1 when the step starts outside the grid (no tally).
-template <class R>
+template <class R, bool BATCH>
 __device__ __forceinline__ int start_step(const Params<R>& P, const Pk<R>& pk, Flight<R>& f, Cnt& c, bool& tflag) {
     ++c.steps;
-    const R kap = P.sc.region[pk.layer].kappa;
+    const R kap = opt_kappa<R, BATCH>(P, pk.inst, pk.layer);
     const R tsdf = f.dsdf * kap;
     f.last = false;
     if (f.taurun + tsdf <= f.tau) {
@@ -342,11 +358,11 @@ __device__ __forceinline__ R face_spacing(R v, R dcomp) {
 }
 
 // One voxel segment of the current step; returns true when the step's walk is over.
-template <class R>
-__device__ __forceinline__ bool walk_segment(const Params<R>& P, const V3<double>& pos, const V3<R>& d, Flight<R>& f,
-                                             Cnt& c, bool& tflag) {
+template <class R, bool BATCH>
+__device__ __forceinline__ bool walk_segment(const Params<R>& P, int inst, const V3<R>& d, Flight<R>& f, Cnt& c,
+                                             bool& tflag) {
     const GridT<R>& g = P.grid;
-    double* const jm = tally_grid(P);
+    double* const jm = tally_grid<R, BATCH>(P, inst);
     const R tm = fmin(f.w.tx, fmin(f.w.ty, f.w.tz));
     const int idx = (f.w.ci - 1) + g.nx * ((f.w.cj - 1) + g.ny * (f.w.ck - 1));
     ++c.vox;
@@ -387,9 +403,9 @@ __device__ __forceinline__ void start_flight(Flight<R>& f, Rng& rng) {
 }
 
 // Moves through a step that starts outside the grid (no walk), then continues.
-template <class R>
+template <class R, bool BATCH>
 __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c) {
-    int a = start_step(P, pk, f, c, pk.tflag);
+    int a = start_step<R, BATCH>(P, pk, f, c, pk.tflag);
     if (a < 0) {
         pk.pos = advance(pk.pos, f.dsdf, pk.dir);
         if (f.last) return end_flight(P, pk);
@@ -404,7 +420,7 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
 // SMCRT_WALK_SEGMENTS voxel segments.  A packet can pass through several
 // actions in one pass (retire -> launch -> sweep -> walk, interact -> sweep ->
 // walk, sweep -> cross).  `c` counts this thread's events since its last flush.
-template <class R, int KERNEL, bool REPLAY>
+template <class R, int KERNEL, bool REPLAY, bool BATCH>
 __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers& B, Pk<R>& pk, Flight<R>& f,
                                                Stream<R, REPLAY>& rng, Cnt& c, int& act, unsigned long long* s_cnt,
                                                double* s_mom, unsigned* s_bins) {
@@ -414,7 +430,8 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // ---- retire a finished packet: detectors (kernelsMod.f90:302-306), counters
     if (act == A_DEATH) {
         if (P.ndet > 0 && KERNEL != SMCRT_KERNEL_TEST)
-            record_detectors(P, B.bins, s_bins, pk.pos.x, pk.pos.y, pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
+            record_detectors(P, BATCH ? B.bins + (long long)pk.inst * P.nbins : B.bins, s_bins, pk.pos.x, pk.pos.y,
+                             pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
                              (double)pk.dir.z, (double)pk.weight, pk.layer + 1);
         // per-packet totals, summed over the retiring lanes first: one shared
         // atomic per warp (a shared-memory FP64 add is a compare-and-swap loop)
@@ -430,6 +447,12 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         if (pk.flags & STATUS_ERROR_STATE) atomicAdd(&s_cnt[C_ERR], 1ull);
         const int fl = pk.flags | rng.flags;
         if (fl) atomicOr(B.status, fl);
+        if (BATCH) {
+            unsigned long long* bs = P.bstats + 3ll * pk.inst;
+            atomicAdd(bs + 0, 1ull);
+            atomicAdd(bs + 1, (unsigned long long)rng.ndraws);
+            atomicAdd(bs + 2, (unsigned long long)pk.nscatt);
+        }
         // this thread's event counts stay in registers until the kernel ends;
         // flushed early only long before they could wrap
         if ((c.sdf | c.vox | c.steps) > (1u << 30)) {
@@ -463,8 +486,23 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         if ((int)lane == leader) base = atomicAdd(B.work, (unsigned long long)__popc(m));
         base = __shfl_sync(m, base, leader);
         const long long pid = (long long)(base + rank);
-        if (pid >= P.count) {
+        const long long total = BATCH ? P.bprefix[P.ninst] : P.count;
+        if (pid >= total) {
             act = A_DONE;
+        } else if (BATCH) {
+            // the instance holding launch packet `pid`: last i with bprefix[i] <= pid
+            int lo = 0, hi = P.ninst - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (P.bprefix[mid] <= pid) lo = mid;
+                else hi = mid - 1;
+            }
+            pk.inst = lo;
+            rng.init(P.bseed[lo], P.instance, (uint64_t)(pid - P.bprefix[lo]), nullptr, 0);
+            emit(P, pk, rng);
+            start_flight(f, rng);
+            f.mode = S_LAUNCH;
+            act = A_SWEEP;
         } else {
             const long long gpid = P.first + pid;
             if (REPLAY) {
@@ -483,9 +521,12 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // ---- between flights (kernelsMod.f90:285-300 / 99-134 / 408-436)
     if (act == A_INTERACT) {
         const DRegion<R>& rg = sc.region[pk.layer];
+        const R albedo = BATCH ? P.bopt[pk.inst].albedo[pk.layer] : rg.albedo;
+        const R hgg = BATCH ? P.bopt[pk.inst].hgg[pk.layer] : rg.hgg;
+        const R g2 = BATCH ? P.bopt[pk.inst].g2[pk.layer] : rg.g2;
         act = A_SWEEP;
         if (KERNEL == SMCRT_KERNEL_WEIGHT) {
-            const R wa = pk.weight * ((R)1 - rg.albedo);
+            const R wa = pk.weight * ((R)1 - albedo);
             pk.weight = pk.weight - wa;
             const R ox = (R)pk.pos.x + P.grid.xmax, oy = (R)pk.pos.y + P.grid.ymax, oz = (R)pk.pos.z + P.grid.zmax;
             const int ci = (int)floor((R)P.grid.nx * ox / ((R)2 * P.grid.xmax)) + 1;
@@ -495,9 +536,9 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 pk.tflag = true;
                 act = A_DEATH;
             } else {
-                atomicAdd(tally_grid(P) + (ci - 1) + (long long)P.grid.nx * ((cj - 1) + (long long)P.grid.ny * (ck - 1)),
+                atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + (ci - 1) + (long long)P.grid.nx * ((cj - 1) + (long long)P.grid.ny * (ck - 1)),
                           (double)wa);
-                pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
+                pk.dir = hg_scatter(pk.dir, hgg, g2, rng);
                 ++c.scat;
                 if (pk.weight < (R)0.01) {  // THRESHOLD, CHANCE (constants.f90:28-30)
                     if (rng.next() < (R)0.1) pk.weight = pk.weight / (R)0.1;
@@ -509,8 +550,8 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             }
         } else {
             const R ran = rng.next();
-            if (ran < rg.albedo) {
-                pk.dir = hg_scatter(pk.dir, rg.hgg, rg.g2, rng);
+            if (ran < albedo) {
+                pk.dir = hg_scatter(pk.dir, hgg, g2, rng);
                 ++c.scat;
                 pk.nscatt += 1;
                 if (KERNEL == SMCRT_KERNEL_TEST) {
@@ -578,7 +619,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 pk.tflag = true;
                 act = end_flight(P, pk);
             } else {
-                act = step_or_skip(P, pk, f, c);
+                act = step_or_skip<R, BATCH>(P, pk, f, c);
             }
         } else if (mode == S_STEP) {
             if (mn >= (R)0) {  // outside every region (:92-96)
@@ -589,7 +630,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 pk.flags |= STATUS_STEP_CAP;
                 act = end_flight(P, pk);
             } else if (mna > eps) {
-                act = step_or_skip(P, pk, f, c);
+                act = step_or_skip<R, BATCH>(P, pk, f, c);
             } else if (f.taurun >= f.tau || pk.tflag) {
                 act = end_flight(P, pk);  // (:99-102)
             } else {
@@ -608,7 +649,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             }
             act = A_CROSS;
             f.mode = S_TOP;
-            if (sc.region[L].nidx != sc.region[nl].nidx) {
+            if (opt_nidx<R, BATCH>(P, pk.inst, L) != opt_nidx<R, BATCH>(P, pk.inst, nl)) {
                 int which = -1;
                 if (dsL < (R)0 && dsN < (R)0) {
                     which = (fabs(dsL) <= fabs(dsN)) ? L : nl;
@@ -648,7 +689,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             c.sdf += 4;
             const V3<double> Nn = calc_normal_cold(P.sc64, which, pk.pos, P.normal_h);
             V3<double> I{(double)pk.dir.x, (double)pk.dir.y, (double)pk.dir.z};
-            const double m1 = P.sc64.region[L].nidx, m2 = P.sc64.region[nl].nidx;
+            const double m1 = opt_nidx64<R, BATCH>(P, pk.inst, L), m2 = opt_nidx64<R, BATCH>(P, pk.inst, nl);
             const double Rf = fresnel(I, Nn, m1, m2);
             const double u = (double)rng.next();
             const bool refl = u <= Rf;
@@ -673,7 +714,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // ---- walk voxel segments: at most SMCRT_WALK_SEGMENTS per lane per
     // iteration, so one long walk does not hold up the other lanes' actions
     for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
-        if (walk_segment(P, pk.pos, pk.dir, f, c, pk.tflag)) {
+        if (walk_segment<R, BATCH>(P, pk.inst, pk.dir, f, c, pk.tflag)) {
             pk.pos = advance(pk.pos, f.dsdf, pk.dir);
             if (f.last) {
                 act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
@@ -725,7 +766,7 @@ struct Slots {
     // act | layer << 3 | mode << 7 | last << 9 | tflag << 10 | pk.flags << 16 | rng.flags << 24
     uint32_t meta[kSlots];
     int steps[kSlots], nscatt[kSlots];
-    uint32_t bl[kSlots];  // bounces | rng.left << 16
+    uint32_t bl[kSlots];  // bounces (<= 1001) | rng.left << 11 | batch instance << 14
     uint32_t p0[kSlots], p1[kSlots], block[kSlots], ndraws[kSlots];
     uint32_t b0[kSlots], b1[kSlots], b2[kSlots], b3[kSlots];
 };
@@ -746,7 +787,7 @@ __device__ __forceinline__ R get_r(const uint32_t (*u)[kSlots], int k, int s) {
     return (R)__longlong_as_double((long long)(((unsigned long long)u[k + 1][s] << 32) | u[k][s]));
 }
 
-template <class R, bool REPLAY>
+template <class R, bool REPLAY, bool BATCH>
 __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params<R>& P, const Buffers& B, Pk<R>& pk,
                                          Flight<R>& f, Stream<R, REPLAY>& rng) {
     const uint32_t m = sl.meta[s];
@@ -757,6 +798,7 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     pk.tflag = (m >> 10) & 1u;
     pk.flags = (int)((m >> 16) & 255u);
     rng.flags = (int)(m >> 24);
+    pk.inst = 0;
     if (act == A_NEW) return act;
     pk.pos = V3<double>{sl.px[s], sl.py[s], sl.pz[s]};
     pk.dir = V3<R>{sl.dx[s], sl.dy[s], sl.dz[s]};
@@ -767,8 +809,9 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     f.steps = sl.steps[s];
     pk.nscatt = sl.nscatt[s];
     const uint32_t bl = sl.bl[s];
-    pk.bounces = (int)(bl & 0xFFFFu);
-    rng.left = (int)(bl >> 16);
+    pk.bounces = (int)(bl & 0x7FFu);
+    rng.left = (int)((bl >> 11) & 7u);
+    pk.inst = (int)(bl >> 14);
     rng.p0 = sl.p0[s];
     rng.p1 = sl.p1[s];
     rng.block = sl.block[s];
@@ -777,7 +820,7 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     rng.b1 = sl.b1[s];
     rng.b2 = sl.b2[s];
     rng.b3 = sl.b3[s];
-    rng.seed = P.seed;
+    rng.seed = BATCH ? P.bseed[pk.inst] : P.seed;  // the stream key: the launch's, or the instance's
     rng.inst = P.instance;
     if (REPLAY) {
         const long long pid = (long long)(((uint64_t)rng.p1 << 32) | rng.p0) - P.first;
@@ -822,7 +865,7 @@ __device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const P
     sl.dsdf[s] = f.dsdf;
     sl.steps[s] = f.steps;
     sl.nscatt[s] = pk.nscatt;
-    sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 16);
+    sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 11) | ((uint32_t)pk.inst << 14);
     sl.p0[s] = rng.p0;
     sl.p1[s] = rng.p1;
     sl.block[s] = rng.block;
@@ -865,7 +908,7 @@ __host__ __device__ constexpr size_t slots_bytes() {
 // works on 32 packets that start the pass with the same action, whatever mix of
 // actions the CTA's packets are in; rare actions (boundary events, retire and
 // launch) are gathered across the CTA instead of stalling 31 idle lanes.
-template <class R, int KERNEL, bool REPLAY>
+template <class R, int KERNEL, bool REPLAY, bool BATCH = false>
 __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
                                                                              const Buffers B) {
     constexpr int Q = SlotCount<R>::per_thread;
@@ -888,6 +931,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     for (int q = 0; q < Q; ++q) sl.meta[t + q * kBlock] = (uint32_t)A_NEW;
 
     Pk<R> pk;
+    pk.inst = 0;
     Flight<R> f;
     Stream<R, REPLAY> rng;
     Cnt c = {0, 0, 0, 0, 0, 0};
@@ -961,8 +1005,8 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         // ---- one pass per listed packet: warp w takes 32-item chunks w, w + NW, ...
         for (int i = t; i < total; i += kBlock) {
             const int s = s_list[i];
-            int act = load_slot(sl, s, P, B, pk, f, rng);
-            transport_pass<R, KERNEL, REPLAY>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins);
+            int act = load_slot<R, REPLAY, BATCH>(sl, s, P, B, pk, f, rng);
+            transport_pass<R, KERNEL, REPLAY, BATCH>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins);
             store_slot(sl, s, act, pk, f, rng);
         }
     }

@@ -193,3 +193,29 @@ def benchmark_settings(name: str) -> Settings:
     else:
         raise ConfigError(f"unknown benchmark configuration {name}")
     return st
+
+
+BATCH_SEED = 20240256
+
+
+def batch_instances(ninst: int = 256, seed: int = BATCH_SEED, scale: float = 1.0):
+    """The batched configuration: `ninst` instances of the box_slab geometry on a
+    64^3 grid, each with mu_a ~ U(0.01, 1), mu_s ~ U(1, 100), g ~ U(0.7, 0.95),
+    n ~ U(1.33, 1.45) for the box (the ambient region keeps AMBIENT) and
+    round(10^U(4, 6) * scale) packets, drawn from numpy's PCG64 with `seed`;
+    instance i uses packet stream seed + i.  Returns (settings, optics (ninst, 2, 4)
+    as (mus, mua, hgg, n), packet counts, stream seeds)."""
+    import numpy as np
+    st = benchmark_settings("box_slab")
+    st.grid.nxg = st.grid.nyg = st.grid.nzg = 64
+    rng = np.random.default_rng(seed)
+    mua = rng.uniform(0.01, 1.0, ninst)
+    mus = rng.uniform(1.0, 100.0, ninst)
+    g = rng.uniform(0.7, 0.95, ninst)
+    n = rng.uniform(1.33, 1.45, ninst)
+    counts = np.maximum(1, np.round(10.0 ** rng.uniform(4.0, 6.0, ninst) * scale)).astype(np.int64)
+    optics = np.zeros((ninst, 2, 4))
+    optics[:, 0] = np.stack([mus, mua, g, n], axis=1)
+    optics[:, 1] = (AMBIENT.mus, AMBIENT.mua, AMBIENT.hgg, AMBIENT.n)
+    seeds = (seed + np.arange(ninst)).astype(np.uint64)
+    return st, optics, counts, seeds

@@ -128,6 +128,115 @@ class Transport:
         return RunResult(self._grid_view(jm), bins, st.to_dict()), states[:n]
 
 
+class Batch:
+    """Many instances of one scene (smcrt_batch_*): shared geometry, grid, source and
+    detectors; per-instance region optics, packet counts and seeds; one persistent
+    launch.  Instance i runs the packets `Transport.run(nphotons[i], seeds[i])` would
+    run with its optics."""
+
+    def __init__(self, array, settings: Settings, ninst: int, *, kernel: str = "pathlength",
+                 precision: str = "fp32", optics=None, timeout_ms: int = 0, instance: int = 0):
+        self.settings = settings
+        self.flat = array if isinstance(array, FlatScene) else FlatScene(array)
+        self.grid = settings.grid_c()
+        self.source = settings.source_c()
+        dets = settings.detectors_c()
+        self._dets = (abi.Detector * max(1, len(dets)))(*dets)
+        o = abi.Options()
+        o.kernel = KERNELS[kernel]
+        o.precision = PRECISIONS[precision]
+        o.timeout_ms = timeout_ms
+        o.instance = instance
+        self.options = o
+        self.ninst = int(ninst)
+        self._b = C.c_void_p()
+        check(lib().smcrt_batch_create(self.flat.ptr(), C.byref(self.grid), C.byref(self.source), self._dets,
+                                       len(dets), C.byref(o), self.ninst, C.byref(self._b)))
+        g = settings.grid
+        self.shape = (g.nxg, g.nyg, g.nzg)
+        self.ncell = g.nxg * g.nyg * g.nzg
+        self.nregions = self.flat.nregions
+        self.nbins = sum((d.nbins + 1) ** (2 if d.type == "camera" else 1) for d in settings.detectors)
+        if optics is not None:
+            self.set_optics(optics)
+
+    def set_optics(self, optics) -> None:
+        """optics: (ninst, nregions, 4) array of (mus, mua, hgg, n) per instance and region."""
+        a = np.ascontiguousarray(optics, dtype=np.float64).reshape(self.ninst, self.nregions, 4)
+        check(lib().smcrt_batch_set_optics(self._b, a.ctypes.data_as(C.POINTER(abi.RegionOptics))))
+
+    def launch(self, nphotons, seeds, use_graph: bool = False) -> None:
+        n = np.ascontiguousarray(nphotons, dtype=np.int64).reshape(self.ninst)
+        sd = np.ascontiguousarray(seeds, dtype=np.uint64).reshape(self.ninst)
+        check(lib().smcrt_batch_launch(self._b, abi.i64ptr(n), sd.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                       int(bool(use_graph))))
+
+    def wait(self, want_jmean: bool = True, jmean_out: np.ndarray | None = None):
+        """(jmean (ninst, nxg, nyg, nzg) Fortran order per instance or None, bins (ninst, nbins),
+        per-instance stats dicts, launch totals).  jmean_out: a flat float64 buffer of
+        ninst * ncell (e.g. pinned) to copy the tallies into."""
+        jm = None
+        if want_jmean:
+            jm = jmean_out if jmean_out is not None else np.empty(self.ninst * self.ncell, dtype=np.float64)
+        bins = np.zeros(max(self.ninst * self.nbins, 1), dtype=np.float64)
+        per = (abi.Stats * self.ninst)()
+        tot = abi.Stats()
+        check(lib().smcrt_batch_wait(self._b, abi.dptr(jm), abi.dptr(bins) if self.nbins else None, per,
+                                     C.byref(tot)))
+        if jm is not None:
+            jm = jm.reshape((self.ninst,) + self.shape[::-1]).transpose(0, 3, 2, 1)
+        return jm, bins[: self.ninst * self.nbins].reshape(self.ninst, self.nbins), \
+            [per[i].to_dict() for i in range(self.ninst)], tot.to_dict()
+
+    def run(self, nphotons, seeds, use_graph: bool = False, want_jmean: bool = True):
+        self.launch(nphotons, seeds, use_graph)
+        return self.wait(want_jmean)
+
+    def device_tallies(self) -> tuple[int, int]:
+        jm, bins = C.c_void_p(), C.c_void_p()
+        check(lib().smcrt_batch_device_tallies(self._b, C.byref(jm), C.byref(bins)))
+        return jm.value, bins.value
+
+    @property
+    def stream(self) -> int:
+        return int(lib().smcrt_batch_stream(self._b))
+
+    def close(self) -> None:
+        if self._b:
+            lib().smcrt_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def run_batched(transports: list, nphotons, seeds):
+    """smcrt_run_batched over Transport contexts: one launch when their scenes share
+    the geometry.  Returns a RunResult per context (stats: packets, rng_draws, nscatt)."""
+    n = len(transports)
+    nph = np.ascontiguousarray(nphotons, dtype=np.int64).reshape(n)
+    sd = np.ascontiguousarray(seeds, dtype=np.uint64).reshape(n)
+    ctxs = (C.c_void_p * n)(*[t._ctx.value for t in transports])
+    jms = [np.empty(t.ncell, dtype=np.float64) for t in transports]
+    bins = [np.zeros(max(t.nbins, 1), dtype=np.float64) for t in transports]
+    jp = (C.POINTER(C.c_double) * n)(*[abi.dptr(a) for a in jms])
+    bp = (C.POINTER(C.c_double) * n)(*[abi.dptr(b) for b in bins])
+    st = (abi.Stats * n)()
+    check(lib().smcrt_run_batched(C.cast(ctxs, C.POINTER(C.c_void_p)), n, abi.i64ptr(nph),
+                                  sd.ctypes.data_as(C.POINTER(C.c_uint64)), jp, bp, st))
+    return [RunResult(t._grid_view(j), b[: t.nbins], st[i].to_dict())
+            for i, (t, j, b) in enumerate(zip(transports, jms, bins))]
+
+
 # ---------------------------------------------------------------------- probes
 def eval_sdf(flat: FlatScene, pts: np.ndarray, precision: str = "fp32") -> np.ndarray:
     pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)

@@ -67,6 +67,7 @@ STRUCTS = {
                                 "fresnel_events", "reflections", "kills_step_cap", "kills_error", "rng_draws",
                                 "moments", "kernel_ms", "device_status"]),
     "smcrt_packet_state": (abi.PacketState, ["pos", "dir", "weight", "layer", "nscatt", "ndraws", "flags"]),
+    "smcrt_region_optics": (abi.RegionOptics, ["mus", "mua", "hgg", "n"]),
 }
 
 
