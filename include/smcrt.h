@@ -237,6 +237,21 @@ int64_t smcrt_detector_bins(const smcrt_ctx* ctx);
 int32_t smcrt_run(smcrt_ctx* ctx, int64_t nphotons, uint64_t seed,
                   double* jmean, double* det_bins, smcrt_stats* stats);
 
+/* Autotuning (no counterpart in the reference).  Times runs of trial_packets
+ * packets of stream `seed` for each candidate launch configuration -- fluence-grid
+ * copies 1, 2, 4, 8 (as many as fit in 256 MiB) x detector bins counted in
+ * shared memory or in global memory -- and keeps the fastest for the context's
+ * later runs.  The CTA shape (640 threads, 2 packet slots per thread) is fixed at
+ * build time.  Overwrites the context's device tallies. */
+typedef struct smcrt_tuning {
+    int32_t tally_copies;  /* chosen fluence-grid copies */
+    int32_t shared_bins;   /* 1: detector bins counted in shared memory */
+    double packets_per_s;  /* measured rate of the chosen configuration */
+    int32_t trials;        /* trial runs made */
+    int32_t reserved;
+} smcrt_tuning;
+int32_t smcrt_autotune(smcrt_ctx* ctx, int64_t trial_packets, uint64_t seed, smcrt_tuning* result);
+
 /* Device-resident form: ADDS the tallies of packets [first, first+count) into
  * caller-owned DEVICE buffers, asynchronously on the context stream.  Used for
  * sharding packet ranges and for timing with data already in HBM.  stats may be

@@ -123,6 +123,11 @@ class RegionOptics(C.Structure):
     _fields_ = [("mus", C.c_double), ("mua", C.c_double), ("hgg", C.c_double), ("n", C.c_double)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("tally_copies", C.c_int32), ("shared_bins", C.c_int32), ("packets_per_s", C.c_double),
+                ("trials", C.c_int32), ("reserved", C.c_int32)]
+
+
 # Exported symbols of include/smcrt.h with their argtypes/restype.
 SIGNATURES = {
     "smcrt_abi_version": ([], C.c_int32),
@@ -140,6 +145,7 @@ SIGNATURES = {
     "smcrt_run_batched": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_uint64),
                            C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_double)), C.POINTER(Stats)],
                           C.c_int32),
+    "smcrt_autotune": ([C.c_void_p, C.c_int64, C.c_uint64, C.POINTER(Tuning)], C.c_int32),
     "smcrt_batch_create": ([C.POINTER(Scene), C.POINTER(Grid), C.POINTER(Source), C.POINTER(Detector), C.c_int32,
                             C.POINTER(Options), C.c_int32, C.POINTER(C.c_void_p)], C.c_int32),
     "smcrt_batch_set_optics": ([C.c_void_p, C.POINTER(RegionOptics)], C.c_int32),

@@ -228,6 +228,8 @@ struct smcrt_ctx {
     Params<double>* pd = nullptr;
     long long ncell = 0, nbins = 0;
     int tcopies = 1;                          // fluence-grid copies (1 = the output grid only)
+    int copies_alloc = 1;                     // copies d_copies holds (+1 for the output grid)
+    bool shared_bins_on = true;               // detector bins counted in shared memory when they fit
     double* d_jmean = nullptr;
     double* d_copies = nullptr;               // tcopies - 1 zeroed copies
     double* d_bins = nullptr;
@@ -373,7 +375,7 @@ int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, doubl
     B.states = d_states;
     long long need = (count + c->block - 1) / c->block;
     int blocks = (int)std::min<long long>(c->grid_blocks, std::max<long long>(need, 1));
-    const int sb = shared_bins(c->nbins, count);
+    const int sb = c->shared_bins_on ? shared_bins(c->nbins, count) : 0;
     int tc = 1;  // a power of two, at most one copy per CTA
     while (tc * 2 <= std::min(c->tcopies, blocks)) tc *= 2;
     int rc;
@@ -545,6 +547,7 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
         CKC(cudaMalloc(&c->d_copies, bytes));
         CKC(cudaMemset(c->d_copies, 0, bytes));  // the reduce kernel re-zeroes after each launch
     }
+    c->copies_alloc = c->tcopies;
     CKC(cudaMalloc(&c->d_bins, sizeof(double) * std::max(1ll, nbins)));
     CKC(cudaMalloc(&c->d_work, sizeof(unsigned long long) * (1 + C_NUM)));
     CKC(cudaMalloc(&c->d_mom, sizeof(double) * 25));
@@ -592,6 +595,67 @@ int32_t smcrt_run_device(smcrt_ctx* c, int64_t first, int64_t count, uint64_t se
     rc = wait_bounded(c);
     if (rc) return rc;
     return read_stats(c, stats);
+}
+
+int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt_tuning* result) {
+    g_err.clear();
+    if (!c || trial_packets < 1) return fail(SMCRT_ERR_ARG, "autotune: bad arguments");
+    // candidates: fluence-grid copies 1, 2, 4, 8 (as many as fit in 256 MiB), detector bins
+    // in shared memory or not (only when there are bins that fit)
+    std::vector<int> copies;
+    for (int k = 1; k <= 8; k *= 2)
+        if (k == 1 || (long long)k * c->ncell * 8 <= (256ll << 20)) copies.push_back(k);
+    const int maxc = copies.back();
+    if (maxc > c->copies_alloc) {
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->d_copies) CK(cudaFree(c->d_copies));
+        c->d_copies = nullptr;
+        const size_t bytes = sizeof(double) * (size_t)(maxc - 1) * (size_t)c->ncell;
+        CK(cudaMalloc(&c->d_copies, bytes));
+        CK(cudaMemset(c->d_copies, 0, bytes));
+        c->copies_alloc = maxc;
+    }
+    std::vector<int> sbins = {1};
+    if (c->nbins > 0 && c->nbins <= kMaxSharedBins) sbins.push_back(0);
+    const int keep_tc = c->tcopies;
+    const bool keep_sb = c->shared_bins_on;
+    double best = -1.0;
+    int best_tc = keep_tc, best_sb = keep_sb, trials = 0;
+    for (int tc : copies)
+        for (int sb : sbins) {
+            c->tcopies = tc;
+            c->shared_bins_on = sb != 0;
+            double best_here = 0.0;
+            for (int rep = 0; rep < 2; ++rep) {  // best of two: the first may pay cold caches
+                CK(cudaMemsetAsync(c->d_jmean, 0, sizeof(double) * c->ncell, c->stream));
+                CK(cudaMemsetAsync(c->d_bins, 0, sizeof(double) * std::max(1ll, c->nbins), c->stream));
+                CK(cudaEventRecord(c->ev0, c->stream));
+                int rc = enqueue(c, 0, trial_packets, seed, c->d_jmean, c->d_bins, false, nullptr, nullptr, nullptr);
+                if (rc) return rc;
+                CK(cudaEventRecord(c->ev1, c->stream));
+                rc = wait_bounded(c);
+                if (rc) return rc;
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+                best_here = std::max(best_here, (double)trial_packets / (ms * 1e-3));
+                ++trials;
+            }
+            if (best_here > best) {
+                best = best_here;
+                best_tc = tc;
+                best_sb = sb;
+            }
+        }
+    c->tcopies = best_tc;
+    c->shared_bins_on = best_sb != 0;
+    if (result) {
+        result->tally_copies = best_tc;
+        result->shared_bins = best_sb;
+        result->packets_per_s = best;
+        result->trials = trials;
+        result->reserved = 0;
+    }
+    return SMCRT_OK;
 }
 
 int32_t smcrt_run(smcrt_ctx* c, int64_t nphotons, uint64_t seed, double* jmean, double* det_bins,

@@ -102,6 +102,14 @@ class Transport:
                               abi.dptr(bins) if self.nbins else None, C.byref(st)))
         return RunResult(self._grid_view(jm) if jm is not None else None, bins, st.to_dict())
 
+    def autotune(self, trial_packets: int = 200000, seed: int = 0) -> dict:
+        """smcrt_autotune: times trial runs of each launch configuration (fluence-grid
+        copies, detector-bin privatisation) and keeps the fastest for later runs."""
+        t = abi.Tuning()
+        check(lib().smcrt_autotune(self._ctx, int(trial_packets), int(seed), C.byref(t)))
+        return {"tally_copies": t.tally_copies, "shared_bins": bool(t.shared_bins),
+                "packets_per_s": t.packets_per_s, "trials": t.trials}
+
     def run_device(self, first: int, count: int, seed: int, jmean_dev: int, bins_dev: int | None,
                    stats: bool = False) -> dict | None:
         """Adds the tallies of packets [first, first+count) into caller-owned device

@@ -68,6 +68,7 @@ STRUCTS = {
                                 "moments", "kernel_ms", "device_status"]),
     "smcrt_packet_state": (abi.PacketState, ["pos", "dir", "weight", "layer", "nscatt", "ndraws", "flags"]),
     "smcrt_region_optics": (abi.RegionOptics, ["mus", "mua", "hgg", "n"]),
+    "smcrt_tuning": (abi.Tuning, ["tally_copies", "shared_bins", "packets_per_s", "trials"]),
 }
 
 

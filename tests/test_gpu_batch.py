@@ -74,3 +74,19 @@ def test_run_batched_over_contexts():
     assert res2[2].stats["packets"] == 1000
     for t in trs + [other]:
         t.close()
+
+
+@pytest.mark.parametrize("cfg", ["box_slab", "layered_vessels"])
+def test_autotune_keeps_results(cfg):
+    """The autotuner only changes how tallies are accumulated: FP64 event counts
+    and tallies of a run are the same before and after tuning."""
+    st = P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+    with Transport(arr, st, precision="fp64") as tr:
+        before = tr.run(20000, 4)
+        t = tr.autotune(trial_packets=50000)
+        after = tr.run(20000, 4)
+    assert t["tally_copies"] in (1, 2, 4, 8) and t["packets_per_s"] > 0 and t["trials"] >= 2
+    assert before.stats["voxel_segments"] == after.stats["voxel_segments"]
+    assert np.array_equal(before.bins, after.bins)
+    np.testing.assert_allclose(after.jmean, before.jmean, rtol=1e-9, atol=1e-12 * before.jmean.max())
