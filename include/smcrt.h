@@ -237,6 +237,23 @@ int64_t smcrt_detector_bins(const smcrt_ctx* ctx);
 int32_t smcrt_run(smcrt_ctx* ctx, int64_t nphotons, uint64_t seed,
                   double* jmean, double* det_bins, smcrt_stats* stats);
 
+/* Adjoint of a pathlength run (no counterpart in the reference): the gradient of
+ *     L = sum_v w[v] * jmean[v] + sum_b h[b] * det_bins[b]
+ * (the raw tallies of smcrt_run(ctx, nphotons, seed)) with respect to every
+ * region group's (mua, mus, g), by path replay: each packet is traced again from
+ * its regenerated stream, twice (its total contribution, then the score terms of
+ * its events), and nothing per packet is stored.  The expected value is exact;
+ * the estimate is the perturbation Monte Carlo (score-function) gradient of the
+ * same packets.  w_dev: FP32 DEVICE array (nxg*nyg*nzg), gbins_dev: FP64 DEVICE
+ * array (smcrt_detector_bins) or NULL; region_group[r] in -1..ngroups-1 ties
+ * region r's parameters to a group (-1: not differentiated), ngroups <= 5.
+ * grad (HOST, 3*ngroups): [d/d mua of groups..., d/d mus..., d/d g...], sums
+ * over packets (divide by nphotons for the per-packet loss).  Needs an FP32
+ * pathlength context. */
+int32_t smcrt_adjoint(smcrt_ctx* ctx, int64_t nphotons, uint64_t seed, const float* w_dev,
+                      const double* gbins_dev, const int32_t* region_group, int32_t ngroups,
+                      double* grad, smcrt_stats* stats);
+
 /* Autotuning (no counterpart in the reference).  Times runs of trial_packets
  * packets of stream `seed` for each candidate launch configuration -- fluence-grid
  * copies 1, 2, 4, 8 (as many as fit in 256 MiB) x detector bins counted in

@@ -145,6 +145,8 @@ SIGNATURES = {
     "smcrt_run_batched": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_uint64),
                            C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_double)), C.POINTER(Stats)],
                           C.c_int32),
+    "smcrt_adjoint": ([C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_int32,
+                       C.POINTER(C.c_double), C.POINTER(Stats)], C.c_int32),
     "smcrt_autotune": ([C.c_void_p, C.c_int64, C.c_uint64, C.POINTER(Tuning)], C.c_int32),
     "smcrt_batch_create": ([C.POINTER(Scene), C.POINTER(Grid), C.POINTER(Source), C.POINTER(Detector), C.c_int32,
                             C.POINTER(Options), C.c_int32, C.POINTER(C.c_void_p)], C.c_int32),

@@ -597,6 +597,60 @@ int32_t smcrt_run_device(smcrt_ctx* c, int64_t first, int64_t count, uint64_t se
     return read_stats(c, stats);
 }
 
+int32_t smcrt_adjoint(smcrt_ctx* c, int64_t nphotons, uint64_t seed, const float* w_dev, const double* gbins_dev,
+                      const int32_t* region_group, int32_t ngroups, double* grad, smcrt_stats* stats) {
+    g_err.clear();
+    if (!c || nphotons < 0 || !w_dev || !region_group || !grad) return fail(SMCRT_ERR_ARG, "adjoint: bad arguments");
+    if (c->precision != SMCRT_FP32 || c->kernel != SMCRT_KERNEL_PATHLENGTH)
+        return fail(SMCRT_ERR_ARG, "adjoint: needs an FP32 pathlength context");
+    if (ngroups < 1 || ngroups > kMaxAdjGroups)
+        return fail(SMCRT_ERR_ARG, "adjoint: 1.." + std::to_string(kMaxAdjGroups) + " parameter groups");
+    Params<float>& P = *c->pf;
+    for (int r = 0; r < P.sc.nregions; ++r) {
+        const int g = region_group[r];
+        if (g < -1 || g >= ngroups) return fail(SMCRT_ERR_ARG, "adjoint: region group out of range");
+        P.adj_group[r] = g < 0 ? 255 : (unsigned char)g;
+    }
+    double* d_out = nullptr;
+    CK(cudaMalloc(&d_out, sizeof(double) * 3 * (size_t)ngroups));
+    auto done = [&](int rc) {
+        cudaFree(d_out);
+        P.adj_w = nullptr;
+        P.adj_gbins = nullptr;
+        P.adj_out = nullptr;
+        P.adj_ngroups = 0;
+        return rc;
+    };
+    if (cudaMemsetAsync(d_out, 0, sizeof(double) * 3 * (size_t)ngroups, c->stream) != cudaSuccess)
+        return done(fail(SMCRT_ERR_CUDA, "adjoint: memset failed"));
+    P.adj_w = w_dev;
+    P.adj_gbins = gbins_dev;
+    P.adj_out = d_out;
+    P.adj_ngroups = ngroups;
+    P.first = 0;
+    P.count = nphotons;
+    P.seed = seed;
+    P.sbins = 0;
+    set_tally_table(&P, c->d_jmean, c->d_copies, 1, c->ncell);
+    if (cudaMemsetAsync(c->d_work, 0, sizeof(unsigned long long) * (1 + C_NUM), c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->d_mom, 0, sizeof(double) * 25, c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream) != cudaSuccess)
+        return done(fail(SMCRT_ERR_CUDA, "adjoint: memset failed"));
+    Buffers B = make_buffers(c, c->d_jmean, c->d_bins);
+    const long long need = (nphotons + kBlock - 1) / kBlock;
+    const int blocks = (int)std::min<long long>(c->grid_blocks, std::max<long long>(need, 1));
+    if (cudaEventRecord(c->ev0, c->stream) != cudaSuccess) return done(fail(SMCRT_ERR_CUDA, "adjoint: event"));
+    cudaError_t e = launch_adjoint_f32_0(P, B, blocks, c->stream);
+    if (e != cudaSuccess) return done(fail(SMCRT_ERR_CUDA, std::string("adjoint launch: ") + cudaGetErrorString(e)));
+    if (cudaEventRecord(c->ev1, c->stream) != cudaSuccess) return done(fail(SMCRT_ERR_CUDA, "adjoint: event"));
+    int rc = wait_bounded(c);
+    if (rc) return done(rc);
+    if (cudaMemcpy(grad, d_out, sizeof(double) * 3 * (size_t)ngroups, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return done(fail(SMCRT_ERR_CUDA, "adjoint: copy failed"));
+    rc = read_stats(c, stats);
+    return done(rc);
+}
+
 int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt_tuning* result) {
     g_err.clear();
     if (!c || trial_packets < 1) return fail(SMCRT_ERR_ARG, "autotune: bad arguments");

@@ -19,6 +19,7 @@ constexpr int kMaxDetectors = 16;
 // larger bin sets (camera images) add straight into the global FP64 bins.
 constexpr int kMaxSharedBins = 4096;
 constexpr int kMaxTallyCopies = 16;
+constexpr int kMaxAdjGroups = 5;  // parameter groups of one adjoint launch (3 parameters each)
 constexpr double kPI = 3.14159265358979323846264338327950288;
 
 // Device status flags (smcrt_stats.device_status).
@@ -55,6 +56,7 @@ template <class R>
 struct DRegion {
     int first, n, op, pad;
     R k, kappa, albedo, hgg, g2, nidx;
+    R mus, mua;  // for the adjoint's scatter/absorption terms
 };
 
 // Optical properties of one batch instance, per region (the per-region fields of
@@ -370,8 +372,10 @@ __device__ __forceinline__ void phi_angles(double u, double& cosp, double& sinp)
     sinp = (u < 0.5) ? s : -s;  // phi = 2 pi u < pi  <=>  u < 1/2
 }
 
+// mu_out: the sampled cos(theta) (the HG variate, before the vertical-case sign
+// rule), for the adjoint's d log p_HG / dg.
 template <class R, class Rng>
-__device__ __forceinline__ V3<R> hg_scatter(V3<R> d, R hgg, R g2, Rng& rng) {
+__device__ __forceinline__ V3<R> hg_scatter(V3<R> d, R hgg, R g2, Rng& rng, R* mu_out = nullptr) {
     const R one = 1;
     R cost, sint;
     if (hgg == (R)0) {
@@ -380,6 +384,7 @@ __device__ __forceinline__ V3<R> hg_scatter(V3<R> d, R hgg, R g2, Rng& rng) {
         (void)rng.next();
         hg_angles(hgg, g2, rng.next(), cost, sint);
     }
+    if (mu_out) *mu_out = cost;
     R cosp, sinp;
     phi_angles(rng.next(), cosp, sinp);
     bool vertical = (one - fabs(d.z) <= (R)1e-12);
@@ -462,6 +467,14 @@ struct Params {
     unsigned long long* bstats;  // [ninst][3]
     int ninst;
     long long nbins;
+    // adjoint launches: d loss / d (per-packet fluence) per voxel, d loss / d
+    // (per-packet detector counts) per bin, the parameter group of each region
+    // (255: none) and the output sums [3][ngroups] (d/d mua, d/d mus, d/d g)
+    const float* adj_w;
+    const double* adj_gbins;
+    double* adj_out;
+    int adj_ngroups;
+    unsigned char adj_group[kMaxRegions];
 };
 
 }  // namespace smcrt

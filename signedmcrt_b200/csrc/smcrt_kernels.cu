@@ -51,6 +51,24 @@ cudaError_t SMCRT_CAT(launch_batch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P
 #endif
 }
 
+// Adjoint launches: FP32 pathlength transport only.
+cudaError_t SMCRT_CAT(launch_adjoint, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, const Buffers& B, int blocks,
+                                                           cudaStream_t s) {
+#if SMCRT_K != 0
+    (void)P; (void)B; (void)blocks; (void)s;
+    return cudaErrorNotSupported;
+#else
+    if (sizeof(SMCRT_R) != 4) return cudaErrorNotSupported;
+    static const cudaError_t attr = cudaFuncSetAttribute(transport_kernel<SMCRT_R, 0, false, false, true>,
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         (int)slots_bytes<SMCRT_R>());
+    if (attr != cudaSuccess) return attr;
+    if (blocks == 0) return cudaSuccess;
+    transport_kernel<SMCRT_R, 0, false, false, true><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
+    return cudaGetLastError();
+#endif
+}
+
 cudaError_t SMCRT_CAT(occupancy, SMCRT_TAG, SMCRT_K)(int block, size_t sbins_bytes, int* per_sm) {
     if (block != kBlock) return cudaErrorInvalidConfiguration;
     cudaError_t e = allow_smem<false>();

@@ -11,7 +11,8 @@ namespace smcrt {
     cudaError_t launch_##TAG##_##K(const Params<R>& P, const Buffers& B, bool replay, int blocks, int block, \
                                    cudaStream_t s);                                                       \
     cudaError_t occupancy_##TAG##_##K(int block, size_t sbins_bytes, int* per_sm);                   \
-    cudaError_t launch_batch_##TAG##_##K(const Params<R>& P, const Buffers& B, int blocks, cudaStream_t s);
+    cudaError_t launch_batch_##TAG##_##K(const Params<R>& P, const Buffers& B, int blocks, cudaStream_t s);   \
+    cudaError_t launch_adjoint_##TAG##_##K(const Params<R>& P, const Buffers& B, int blocks, cudaStream_t s);
 
 SMCRT_DECL_VARIANT(float, f32, 0)
 SMCRT_DECL_VARIANT(float, f32, 1)

@@ -33,6 +33,8 @@ void fill_scene(SceneT<R>& d, const smcrt_scene* s) {
         r.hgg = (R)g.hgg;
         r.g2 = (R)(g.hgg * g.hgg);
         r.nidx = (R)g.n;
+        r.mus = (R)g.mus;
+        r.mua = (R)g.mua;
     }
 }
 template void fill_scene<float>(SceneT<float>&, const smcrt_scene*);

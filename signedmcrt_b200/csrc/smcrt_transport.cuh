@@ -14,6 +14,12 @@
 
 namespace smcrt {
 
+// Threads per CTA of the transport kernel (one CTA per SM).
+#ifndef SMCRT_BLOCK
+#define SMCRT_BLOCK 640
+#endif
+constexpr int kBlock = SMCRT_BLOCK;
+
 enum CounterIdx {
     C_PACKETS = 0,
     C_SDF,
@@ -55,6 +61,8 @@ struct Pk {
     int nscatt;
     int flags;
     int inst;  // batch instance (0 outside batches)
+    int phase;        // adjoint: 0 = first pass (sum C), 1 = second pass (gradient terms)
+    float ctot, cpre; // adjoint: the packet's loss contribution C, and the part of it made so far
     bool tflag;
 };
 
@@ -358,32 +366,41 @@ __device__ __forceinline__ R face_spacing(R v, R dcomp) {
 }
 
 // One voxel segment of the current step; returns true when the step's walk is over.
-template <class R, bool BATCH>
-__device__ __forceinline__ bool walk_segment(const Params<R>& P, int inst, const V3<R>& d, Flight<R>& f, Cnt& c,
-                                             bool& tflag) {
+// (ADJ: the adjoint's track terms instead of the fluence tally; on leaving the
+// grid the rest of the step, untallied, still counts for survival.)
+template <class R, bool BATCH, bool ADJ>
+__device__ __forceinline__ bool walk_segment(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c, float* acc) {
     const GridT<R>& g = P.grid;
-    double* const jm = tally_grid<R, BATCH>(P, inst);
+    const V3<R>& d = pk.dir;
     const R tm = fmin(f.w.tx, fmin(f.w.ty, f.w.tz));
     const int idx = (f.w.ci - 1) + g.nx * ((f.w.cj - 1) + g.ny * (f.w.ck - 1));
     ++c.vox;
     if (tm > f.dsdf) {
-        atomicAdd(jm + idx, (double)(f.dsdf - f.w.td));
+        if (ADJ) adj_track(P, pk, acc, (float)(f.dsdf - f.w.td), P.adj_w[idx]);
+        else atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + idx, (double)(f.dsdf - f.w.td));
         return true;
     }
-    atomicAdd(jm + idx, (double)(tm - f.w.td));
+    if (ADJ) adj_track(P, pk, acc, (float)(tm - f.w.td), P.adj_w[idx]);
+    else atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + idx, (double)(tm - f.w.td));
     f.w.td = tm;
+    bool out = false;
     if (tm == f.w.tx) {
         f.w.ci += d.x > (R)0 ? 1 : -1;
-        if (f.w.ci < 1 || f.w.ci > g.nx) { tflag = true; return true; }
+        out = f.w.ci < 1 || f.w.ci > g.nx;
         f.w.tx = tm + face_spacing(g.vx, d.x);
     } else if (tm == f.w.ty) {
         f.w.cj += d.y > (R)0 ? 1 : -1;
-        if (f.w.cj < 1 || f.w.cj > g.ny) { tflag = true; return true; }
+        out = f.w.cj < 1 || f.w.cj > g.ny;
         f.w.ty = tm + face_spacing(g.vy, d.y);
     } else {
         f.w.ck += d.z > (R)0 ? 1 : -1;
-        if (f.w.ck < 1 || f.w.ck > g.nz) { tflag = true; return true; }
+        out = f.w.ck < 1 || f.w.ck > g.nz;
         f.w.tz = tm + face_spacing(g.vz, d.z);
+    }
+    if (out) {
+        pk.tflag = true;
+        if (ADJ) adj_track(P, pk, acc, (float)(f.dsdf - tm), 0.0f);
+        return true;
     }
     return false;
 }
@@ -396,6 +413,84 @@ __device__ __forceinline__ int end_flight(const Params<R>& P, Pk<R>& pk) {
     return pk.tflag ? A_DEATH : A_INTERACT;
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint (pathlength kernel).  For a loss L = sum_v w_v phi_v + sum_b h_b D_b
+// over per-packet fluence phi and detector counts D, dL/dtheta = E[f x d log p /
+// dtheta] (score function / perturbation Monte Carlo), where f is the packet's
+// contribution and p its path density: per unit path length in region r the
+// survival exp(-(mus_r + mua_r) l), per scatter mus_r p_HG(cos; g_r), per
+// absorption mua_r (the collision density kappa times the albedo test).  By
+// causality each score term only pairs with the contributions made after it, so
+// each packet is traced twice from its regenerated stream: pass 1 sums its total
+// contribution C, pass 2 adds (d log p_e / d theta) x (C - contributions so far)
+// at every event e.  A packet carries two numbers instead of one score per
+// parameter.  Terms go to per-thread accumulators acc[k][group][thread], k = 0
+// d/d mua, 1 d/d mus, 2 d/d g, for the region's parameter group.
+__device__ __forceinline__ void adj_add(float* acc, int k, int grp, float v) {
+    acc[(k * kMaxAdjGroups + grp) * kBlock + threadIdx.x] += v;
+}
+
+// Path length `len` in the packet's region, over which the fluence weight is w
+// (0 where nothing is tallied): survival term and contribution.
+template <class R>
+__device__ __forceinline__ void adj_track(const Params<R>& P, Pk<R>& pk, float* acc, float len, float w) {
+    if (pk.phase == 0) {
+        pk.ctot += w * len;
+        return;
+    }
+    const int grp = P.adj_group[pk.layer];
+    if (grp < P.adj_ngroups) {
+        // integral over the length of -(contributions after each point); the same
+        // for mua and mus (d kappa / d mua = d kappa / d mus = 1)
+        const float v = len * (pk.ctot - pk.cpre) - 0.5f * w * len * len;
+        adj_add(acc, 0, grp, -v);
+        adj_add(acc, 1, grp, -v);
+    }
+    pk.cpre += w * len;
+}
+
+// A scatter in the packet's region with HG variate mu (second pass).
+template <class R>
+__device__ __forceinline__ void adj_scatter(const Params<R>& P, const Pk<R>& pk, float* acc, R mu) {
+    const int grp = P.adj_group[pk.layer];
+    if (grp >= P.adj_ngroups) return;
+    const DRegion<R>& rg = P.sc.region[pk.layer];
+    const float F = pk.ctot - pk.cpre;
+    if ((float)rg.mua < 1e-9f) {  // albedo 1 (init_mono): the interaction density is kappa
+        adj_add(acc, 0, grp, F / (float)rg.kappa);
+        adj_add(acc, 1, grp, F / (float)rg.kappa);
+    } else {
+        adj_add(acc, 1, grp, F / (float)rg.mus);
+    }
+    // d log p_HG(mu; g) / dg, p_HG = (1 - g^2) / (2 (1 + g^2 - 2 g mu)^1.5)
+    const float g = (float)rg.hgg, m = (float)mu;
+    const float den = (1.0f - g) * (1.0f - g) + 2.0f * g * (1.0f - m);  // 1 + g^2 - 2 g mu
+    adj_add(acc, 2, grp, F * (-2.0f * g / (1.0f - g * g) - 3.0f * (g - m) / den));
+}
+
+// An absorption in the packet's region (second pass).
+template <class R>
+__device__ __forceinline__ void adj_absorb(const Params<R>& P, const Pk<R>& pk, float* acc) {
+    const int grp = P.adj_group[pk.layer];
+    if (grp >= P.adj_ngroups) return;
+    adj_add(acc, 0, grp, (pk.ctot - pk.cpre) / (float)P.sc.region[pk.layer].mua);
+}
+
+// Detector part of a retiring packet's contribution: sum of h_b over its bins.
+template <class R>
+__device__ __forceinline__ float adj_detector_term(const Params<R>& P, const Pk<R>& pk) {
+    if (P.ndet == 0 || !P.adj_gbins) return 0.0f;
+    const double p[3] = {pk.pos.x, pk.pos.y, pk.pos.z};
+    const double l[3] = {(double)pk.dir.x, (double)pk.dir.y, (double)pk.dir.z};
+    const double value = sqrt(pk.pos.x * pk.pos.x + pk.pos.y * pk.pos.y);
+    double sum = 0.0;
+    for (int d = 0; d < P.ndet; ++d) {
+        const long long b = detector_bin(P.det[d], p, l, value, pk.layer + 1);
+        if (b >= 0) sum += P.adj_gbins[b];
+    }
+    return (float)sum;
+}
+
 template <class R, class Rng>
 __device__ __forceinline__ void start_flight(Flight<R>& f, Rng& rng) {
     f.tau = -log(rng.next());  // inttau2.f90:46
@@ -403,10 +498,11 @@ __device__ __forceinline__ void start_flight(Flight<R>& f, Rng& rng) {
 }
 
 // Moves through a step that starts outside the grid (no walk), then continues.
-template <class R, bool BATCH>
-__device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c) {
+template <class R, bool BATCH, bool ADJ>
+__device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c, float* acc) {
     int a = start_step<R, BATCH>(P, pk, f, c, pk.tflag);
     if (a < 0) {
+        if (ADJ) adj_track(P, pk, acc, (float)f.dsdf, 0.0f);  // a step outside the grid
         pk.pos = advance(pk.pos, f.dsdf, pk.dir);
         if (f.last) return end_flight(P, pk);
         f.mode = S_STEP;
@@ -420,16 +516,28 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
 // SMCRT_WALK_SEGMENTS voxel segments.  A packet can pass through several
 // actions in one pass (retire -> launch -> sweep -> walk, interact -> sweep ->
 // walk, sweep -> cross).  `c` counts this thread's events since its last flush.
-template <class R, int KERNEL, bool REPLAY, bool BATCH>
+template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ>
 __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers& B, Pk<R>& pk, Flight<R>& f,
                                                Stream<R, REPLAY>& rng, Cnt& c, int& act, unsigned long long* s_cnt,
-                                               double* s_mom, unsigned* s_bins) {
+                                               double* s_mom, unsigned* s_bins, float* acc) {
     const SceneT<R>& sc = P.sc;
     const int N = sc.nregions;
     const R eps = P.eps;
+    // ---- adjoint: the end of a packet's first pass -- add its detector term to C
+    // and trace the same packet again from its regenerated stream
+    if (ADJ && act == A_DEATH && pk.phase == 0) {
+        pk.ctot += adj_detector_term(P, pk);
+        rng.init(rng.seed, rng.inst, ((uint64_t)rng.p1 << 32) | rng.p0, nullptr, 0);
+        emit(P, pk, rng);
+        start_flight(f, rng);
+        f.mode = S_LAUNCH;
+        pk.phase = 1;
+        pk.cpre = 0.0f;
+        act = A_SWEEP;
+    }
     // ---- retire a finished packet: detectors (kernelsMod.f90:302-306), counters
     if (act == A_DEATH) {
-        if (P.ndet > 0 && KERNEL != SMCRT_KERNEL_TEST)
+        if (!ADJ && P.ndet > 0 && KERNEL != SMCRT_KERNEL_TEST)
             record_detectors(P, BATCH ? B.bins + (long long)pk.inst * P.nbins : B.bins, s_bins, pk.pos.x, pk.pos.y,
                              pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
                              (double)pk.dir.z, (double)pk.weight, pk.layer + 1);
@@ -511,6 +619,11 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             } else {
                 rng.init(P.seed, P.instance, (uint64_t)gpid, nullptr, 0);
             }
+            if (ADJ) {
+                pk.phase = 0;
+                pk.ctot = 0.0f;
+                pk.cpre = 0.0f;
+            }
             emit(P, pk, rng);
             start_flight(f, rng);
             f.mode = S_LAUNCH;
@@ -551,7 +664,9 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         } else {
             const R ran = rng.next();
             if (ran < albedo) {
-                pk.dir = hg_scatter(pk.dir, hgg, g2, rng);
+                R mu = 0;
+                pk.dir = hg_scatter(pk.dir, hgg, g2, rng, ADJ ? &mu : nullptr);
+                if (ADJ && pk.phase) adj_scatter(P, pk, acc, mu);
                 ++c.scat;
                 pk.nscatt += 1;
                 if (KERNEL == SMCRT_KERNEL_TEST) {
@@ -569,6 +684,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                     }
                 }
             } else {
+                if (ADJ && pk.phase) adj_absorb(P, pk, acc);
                 pk.tflag = true;
                 act = A_DEATH;
             }
@@ -619,7 +735,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 pk.tflag = true;
                 act = end_flight(P, pk);
             } else {
-                act = step_or_skip<R, BATCH>(P, pk, f, c);
+                act = step_or_skip<R, BATCH, ADJ>(P, pk, f, c, acc);
             }
         } else if (mode == S_STEP) {
             if (mn >= (R)0) {  // outside every region (:92-96)
@@ -630,7 +746,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 pk.flags |= STATUS_STEP_CAP;
                 act = end_flight(P, pk);
             } else if (mna > eps) {
-                act = step_or_skip<R, BATCH>(P, pk, f, c);
+                act = step_or_skip<R, BATCH, ADJ>(P, pk, f, c, acc);
             } else if (f.taurun >= f.tau || pk.tflag) {
                 act = end_flight(P, pk);  // (:99-102)
             } else {
@@ -714,7 +830,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // ---- walk voxel segments: at most SMCRT_WALK_SEGMENTS per lane per
     // iteration, so one long walk does not hold up the other lanes' actions
     for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
-        if (walk_segment<R, BATCH>(P, pk.inst, pk.dir, f, c, pk.tflag)) {
+        if (walk_segment<R, BATCH, ADJ>(P, pk, f, c, acc)) {
             pk.pos = advance(pk.pos, f.dsdf, pk.dir);
             if (f.last) {
                 act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
@@ -734,10 +850,6 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
 #ifndef SMCRT_SLOTS_PER_THREAD
 #define SMCRT_SLOTS_PER_THREAD 2
 #endif
-#ifndef SMCRT_BLOCK
-#define SMCRT_BLOCK 640
-#endif
-constexpr int kBlock = SMCRT_BLOCK;
 // Slots per thread: two for FP32 transport (132 bytes a slot); one for FP64
 // (172 bytes), so that a CTA's slots stay within the 227 KiB of shared memory.
 template <class R>
@@ -763,12 +875,14 @@ struct Slots {
     R dx[kSlots], dy[kSlots], dz[kSlots], w[kSlots];
     R tau[kSlots], taurun[kSlots], dsdf[kSlots];
     uint32_t u[kUW][kSlots];
-    // act | layer << 3 | mode << 7 | last << 9 | tflag << 10 | pk.flags << 16 | rng.flags << 24
+    // act | layer << 3 | mode << 7 | last << 9 | tflag << 10 | adjoint pass << 11 |
+    // pk.flags << 16 | rng.flags << 24
     uint32_t meta[kSlots];
     int steps[kSlots], nscatt[kSlots];
     uint32_t bl[kSlots];  // bounces (<= 1001) | rng.left << 11 | batch instance << 14
     uint32_t p0[kSlots], p1[kSlots], block[kSlots], ndraws[kSlots];
     uint32_t b0[kSlots], b1[kSlots], b2[kSlots], b3[kSlots];
+    float ctot[kSlots], cpre[kSlots];  // adjoint launches only
 };
 
 template <class R, int kSlots>
@@ -787,7 +901,7 @@ __device__ __forceinline__ R get_r(const uint32_t (*u)[kSlots], int k, int s) {
     return (R)__longlong_as_double((long long)(((unsigned long long)u[k + 1][s] << 32) | u[k][s]));
 }
 
-template <class R, bool REPLAY, bool BATCH>
+template <class R, bool REPLAY, bool BATCH, bool ADJ>
 __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params<R>& P, const Buffers& B, Pk<R>& pk,
                                          Flight<R>& f, Stream<R, REPLAY>& rng) {
     const uint32_t m = sl.meta[s];
@@ -796,6 +910,7 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     f.mode = (int)((m >> 7) & 3u);
     f.last = (m >> 9) & 1u;
     pk.tflag = (m >> 10) & 1u;
+    pk.phase = ADJ ? (int)((m >> 11) & 1u) : 0;
     pk.flags = (int)((m >> 16) & 255u);
     rng.flags = (int)(m >> 24);
     pk.inst = 0;
@@ -811,7 +926,7 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     const uint32_t bl = sl.bl[s];
     pk.bounces = (int)(bl & 0x7FFu);
     rng.left = (int)((bl >> 11) & 7u);
-    pk.inst = (int)(bl >> 14);
+    pk.inst = BATCH ? (int)(bl >> 14) : 0;
     rng.p0 = sl.p0[s];
     rng.p1 = sl.p1[s];
     rng.block = sl.block[s];
@@ -821,6 +936,10 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     rng.b2 = sl.b2[s];
     rng.b3 = sl.b3[s];
     rng.seed = BATCH ? P.bseed[pk.inst] : P.seed;  // the stream key: the launch's, or the instance's
+    if (ADJ) {
+        pk.ctot = sl.ctot[s];
+        pk.cpre = sl.cpre[s];
+    }
     rng.inst = P.instance;
     if (REPLAY) {
         const long long pid = (long long)(((uint64_t)rng.p1 << 32) | rng.p0) - P.first;
@@ -847,11 +966,12 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     return act;
 }
 
-template <class R, bool REPLAY>
+template <class R, bool REPLAY, bool BATCH, bool ADJ>
 __device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const Pk<R>& pk, const Flight<R>& f,
                                            const Stream<R, REPLAY>& rng) {
     sl.meta[s] = (uint32_t)act | ((uint32_t)pk.layer << 3) | ((uint32_t)f.mode << 7) | ((uint32_t)f.last << 9) |
-                 ((uint32_t)pk.tflag << 10) | ((uint32_t)pk.flags << 16) | ((uint32_t)rng.flags << 24);
+                 ((uint32_t)pk.tflag << 10) | ((uint32_t)(ADJ ? pk.phase & 1 : 0) << 11) | ((uint32_t)pk.flags << 16) |
+                 ((uint32_t)rng.flags << 24);
     if (act == A_DONE) return;
     sl.px[s] = pk.pos.x;
     sl.py[s] = pk.pos.y;
@@ -865,7 +985,7 @@ __device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const P
     sl.dsdf[s] = f.dsdf;
     sl.steps[s] = f.steps;
     sl.nscatt[s] = pk.nscatt;
-    sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 11) | ((uint32_t)pk.inst << 14);
+    sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 11) | ((uint32_t)(BATCH ? pk.inst : 0) << 14);
     sl.p0[s] = rng.p0;
     sl.p1[s] = rng.p1;
     sl.block[s] = rng.block;
@@ -874,6 +994,10 @@ __device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const P
     sl.b1[s] = rng.b1;
     sl.b2[s] = rng.b2;
     sl.b3[s] = rng.b3;
+    if (ADJ) {
+        sl.ctot[s] = pk.ctot;
+        sl.cpre[s] = pk.cpre;
+    }
     constexpr int W = Slots<R>::kRW;
     if (act == A_WALK) {
         put_r<R>(sl.u, 0, s, f.w.tx);
@@ -908,7 +1032,7 @@ __host__ __device__ constexpr size_t slots_bytes() {
 // works on 32 packets that start the pass with the same action, whatever mix of
 // actions the CTA's packets are in; rare actions (boundary events, retire and
 // launch) are gathered across the CTA instead of stalling 31 idle lanes.
-template <class R, int KERNEL, bool REPLAY, bool BATCH = false>
+template <class R, int KERNEL, bool REPLAY, bool BATCH = false, bool ADJ = false>
 __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
                                                                              const Buffers B) {
     constexpr int Q = SlotCount<R>::per_thread;
@@ -930,8 +1054,14 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
 #pragma unroll
     for (int q = 0; q < Q; ++q) sl.meta[t + q * kBlock] = (uint32_t)A_NEW;
 
+    // adjoint: per-thread gradient accumulators [3][kMaxAdjGroups][kBlock]
+    __shared__ float s_acc[ADJ ? 3 * kMaxAdjGroups * kBlock : 1];
+    if (ADJ)
+        for (int i = t; i < 3 * kMaxAdjGroups * kBlock; i += kBlock) s_acc[i] = 0.0f;
     Pk<R> pk;
     pk.inst = 0;
+    pk.phase = 0;
+    pk.ctot = pk.cpre = 0.0f;
     Flight<R> f;
     Stream<R, REPLAY> rng;
     Cnt c = {0, 0, 0, 0, 0, 0};
@@ -1005,9 +1135,9 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         // ---- one pass per listed packet: warp w takes 32-item chunks w, w + NW, ...
         for (int i = t; i < total; i += kBlock) {
             const int s = s_list[i];
-            int act = load_slot<R, REPLAY, BATCH>(sl, s, P, B, pk, f, rng);
-            transport_pass<R, KERNEL, REPLAY, BATCH>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins);
-            store_slot(sl, s, act, pk, f, rng);
+            int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
+            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc);
+            store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
         }
     }
     // events of packets still in flight (time budget) and since the last retire
@@ -1022,6 +1152,13 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     if (t < 25 && s_mom[t] != 0.0) atomicAdd(B.moments + t, s_mom[t]);
     for (int i = t; i < P.sbins; i += kBlock)
         if (s_bins[i]) atomicAdd(B.bins + i, (double)s_bins[i]);
+    if (ADJ && t < 3 * P.adj_ngroups) {  // thread (k, group) sums its row over the CTA's threads
+        const int k = t / P.adj_ngroups, grp = t % P.adj_ngroups;
+        const float* row = s_acc + (k * kMaxAdjGroups + grp) * kBlock;
+        double sum = 0.0;
+        for (int i = 0; i < kBlock; ++i) sum += (double)row[i];
+        atomicAdd(P.adj_out + k * P.adj_ngroups + grp, sum);
+    }
 }
 
 }  // namespace smcrt

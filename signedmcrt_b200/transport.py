@@ -102,6 +102,22 @@ class Transport:
                               abi.dptr(bins) if self.nbins else None, C.byref(st)))
         return RunResult(self._grid_view(jm) if jm is not None else None, bins, st.to_dict())
 
+    def adjoint(self, nphotons: int, seed: int, w_dev: int, gbins_dev: int | None, region_group,
+                ngroups: int) -> tuple[np.ndarray, dict]:
+        """smcrt_adjoint: d/d(mua, mus, g) of each region group of
+        L = sum_v w[v] jmean[v] + sum_b h[b] bins[b] for the packets of run(nphotons, seed).
+        w_dev / gbins_dev: device pointers (FP32 voxel weights, FP64 bin weights or None).
+        Returns (grad (3, ngroups): rows d/d mua, d/d mus, d/d g, summed over packets; stats)."""
+        rg = np.ascontiguousarray(region_group, dtype=np.int32)
+        if len(rg) != self.flat.nregions:
+            raise ValueError("region_group needs one entry per region")
+        out = np.zeros(3 * ngroups, dtype=np.float64)
+        st = abi.Stats()
+        check(lib().smcrt_adjoint(self._ctx, int(nphotons), int(seed), C.c_void_p(w_dev),
+                                  C.c_void_p(gbins_dev) if gbins_dev else None, abi.i32ptr(rg), int(ngroups),
+                                  abi.dptr(out), C.byref(st)))
+        return out.reshape(3, ngroups), st.to_dict()
+
     def autotune(self, trial_packets: int = 200000, seed: int = 0) -> dict:
         """smcrt_autotune: times trial runs of each launch configuration (fluence-grid
         copies, detector-bin privatisation) and keeps the fastest for later runs."""
