@@ -270,6 +270,94 @@ def run_batch(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args) -> None:
+    """adjoint: layered_vessels, 1e7 packets; the path-replay gradient of a
+    voxel-weighted fluence + detector loss w.r.t. 15 parameters (mu_a, mu_s, g of
+    vessels, 3 layers, bounding medium) -- its cost against the forward launch on
+    the same packets, and its agreement with common-random-number central finite
+    differences (h = 1e-3 relative) over independent batches."""
+    import torch
+    from signedmcrt_b200 import presets as P
+    from signedmcrt_b200.autograd import layered_groups
+    from signedmcrt_b200.transport import Transport
+    if int(os.environ.get("RANK", "0")) != 0 or args.impl == "reference":
+        if args.impl == "reference" and int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no gradient path"}), flush=True)
+        return
+    n = int(args.packets) if args.packets else 10_000_000
+    st = P.benchmark_settings("layered_vessels")
+    scene_fn, groups = layered_groups()
+    base = np.array([[5.0, 50.0, 0.9], [1.0, 100.0, 0.8], [0.3, 50.0, 0.9], [0.1, 30.0, 0.9], [0.01, 0.1, 0.5]])
+    dev = torch.device("cuda", 0)
+    tr = Transport(scene_fn(base), st, precision="fp32", timeout_ms=600000)
+    nx, ny, nz = tr.shape
+    wz = np.linspace(1.0, 0.2, nz)
+    w_host = np.broadcast_to(wz.reshape(1, 1, nz), (nx, ny, nz))
+    w = torch.tensor(np.asfortranarray(w_host).reshape(-1, order="F"), dtype=torch.float32, device=dev)
+    h = torch.linspace(1.0, 2.0, tr.nbins, dtype=torch.float64, device=dev)
+    jm = torch.zeros(tr.ncell, dtype=torch.float64, device=dev)
+    bins = torch.zeros(max(tr.nbins, 1), dtype=torch.float64, device=dev)
+
+    def loss_of(t, count, seed):
+        jm.zero_()
+        bins.zero_()
+        st_ = t.run_device(0, count, seed, jm.data_ptr(), bins.data_ptr(), stats=True)
+        return float((w.double() * jm).sum() + (h * bins[: t.nbins]).sum()) / count, st_["kernel_ms"]
+
+    for wu in range(args.warmup):
+        loss_of(tr, n, 7000 + wu)
+        tr.adjoint(n, 7100 + wu, w.data_ptr(), h.data_ptr(), groups, 5)
+    fwd_ms, adj_ms = [], []
+    for k in range(args.steps):
+        fwd_ms.append(loss_of(tr, n, 11 + k)[1])
+        adj_ms.append(tr.adjoint(n, 11 + k, w.data_ptr(), h.data_ptr(), groups, 5)[1]["kernel_ms"])
+    f_ms, a_ms = sum(fwd_ms) / len(fwd_ms), sum(adj_ms) / len(adj_ms)
+    # finite-difference check on B independent batches of n / B packets
+    B = max(2, args.fd_batches)
+    nb = n // B
+    rel = args.fd_h
+    pert = []
+    for k in range(base.size):
+        dp = np.zeros(base.size)
+        dp[k] = rel * base.flat[k]
+        pert.append((Transport(scene_fn(base + dp.reshape(base.shape)), st, precision="fp32"),
+                     Transport(scene_fn(base - dp.reshape(base.shape)), st, precision="fp32"), dp[k]))
+    adj, fd = [], []
+    for b in range(B):
+        seed = 900 + b
+        g, _ = tr.adjoint(nb, seed, w.data_ptr(), h.data_ptr(), groups, 5)
+        adj.append((g / nb).T.reshape(-1))
+        fd.append([(loss_of(tp, nb, seed)[0] - loss_of(tm, nb, seed)[0]) / (2 * d) for tp, tm, d in pert])
+    for tp, tm, _ in pert:
+        tp.close()
+        tm.close()
+    tr.close()
+    adj, fd = np.array(adj), np.array(fd)
+    se = np.sqrt(adj.var(axis=0, ddof=1) / B + fd.var(axis=0, ddof=1) / B)
+    z = (adj.mean(axis=0) - fd.mean(axis=0)) / np.maximum(se, 1e-300)
+    # a finite difference is informative where the batches see the parameter at all
+    # (not only through FP rounding of the loss): |fd| above 1e-9 of the largest
+    informative = np.abs(fd).max(axis=0) > 1e-9 * np.abs(fd).max()
+    names = [f"{p}_{g}" for g in ("vessel", "layer1", "layer2", "layer3", "bounding") for p in ("mua", "mus", "g")]
+    line = {"metric": "adjoint grad cost vs forward (same packets)", "value": a_ms / f_ms, "unit": "x forward",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": a_ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "layered_vessels, loss = depth-weighted fluence + linearly weighted annulus bins",
+                       "packets": n, "parameters": 15, "groups": "vessels, layer1, layer2, layer3, bounding medium"},
+            "forward_ms": f_ms, "adjoint_ms": a_ms,
+            "fd_check": {"h_rel": rel, "batches": B, "packets_per_batch": nb,
+                         "adjoint": dict(zip(names, adj.mean(axis=0).tolist())),
+                         "fd": dict(zip(names, fd.mean(axis=0).tolist())),
+                         "z": dict(zip(names, z.tolist())),
+                         "adjoint_se": dict(zip(names, (adj.std(axis=0, ddof=1) / np.sqrt(B)).tolist())),
+                         "fd_se": dict(zip(names, (fd.std(axis=0, ddof=1) / np.sqrt(B)).tolist())),
+                         "fd_informative": dict(zip(names, informative.tolist())),
+                         "within_2sigma": int((np.abs(z[informative]) < 2).sum()),
+                         "informative": int(informative.sum())},
+            "gpu_launches": 2 * args.steps}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -277,7 +365,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="sphere_water",
-                    choices=["sphere_water", "box_slab", "layered_vessels", "batch256"])
+                    choices=["sphere_water", "box_slab", "layered_vessels", "batch256", "adjoint"])
+    ap.add_argument("--fd-batches", type=int, default=8, help="adjoint: batches of the finite-difference check")
+    ap.add_argument("--fd-h", type=float, default=1e-3, help="adjoint: relative finite-difference step")
     ap.add_argument("--batch-scale", type=float, default=1.0, help="batch256: packet counts x this factor")
     ap.add_argument("--packets", type=float, default=0, help="packets per GPU per step (default: the config's)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
@@ -293,6 +383,9 @@ def main() -> None:
     from signedmcrt_b200.scene import FlatScene
     if args.config == "batch256":
         run_batch(args)
+        return
+    if args.config == "adjoint":
+        run_adjoint(args)
         return
     st = P.benchmark_settings(args.config)
     arr = P.setup_simulation(st)
