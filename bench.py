@@ -365,7 +365,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="sphere_water",
-                    choices=["sphere_water", "box_slab", "layered_vessels", "batch256", "adjoint"])
+                    choices=["sphere_water", "box_slab", "layered_vessels", "batch256", "adjoint", "accuracy"])
     ap.add_argument("--fd-batches", type=int, default=8, help="adjoint: batches of the finite-difference check")
     ap.add_argument("--fd-h", type=float, default=1e-3, help="adjoint: relative finite-difference step")
     ap.add_argument("--batch-scale", type=float, default=1.0, help="batch256: packet counts x this factor")
@@ -386,6 +386,12 @@ def main() -> None:
         return
     if args.config == "adjoint":
         run_adjoint(args)
+        return
+    if args.config == "accuracy":
+        if int(os.environ.get("RANK", "0")) == 0 and args.impl != "reference":
+            from signedmcrt_b200.accuracy import error_table
+            for cfg, n in (("box_slab", 1_000_000), ("sphere_water", 10_000_000), ("layered_vessels", 10_000_000)):
+                print(json.dumps(error_table(cfg, int(args.packets) if args.packets else n)), flush=True)
         return
     st = P.benchmark_settings(args.config)
     arr = P.setup_simulation(st)

@@ -277,7 +277,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #endif
 
 // Per-lane actions of the flattened transport loop.
-enum Act : int { A_NEW = 0, A_SWEEP, A_WALK, A_CROSS, A_INTERACT, A_DEATH, A_DONE };
+// A_PRECISE (FP32 transport): a sweep within 2 eps of a surface, or resolving a
+// crossing, deferred to the next round and done in FP64 with the other such packets.
+enum Act : int { A_NEW = 0, A_SWEEP, A_WALK, A_CROSS, A_INTERACT, A_DEATH, A_DONE, A_PRECISE };
 // What the next sweep is for.
 enum SweepMode : int { S_LAUNCH = 0, S_TOP, S_STEP, S_CROSS };
 
@@ -301,6 +303,38 @@ struct Flight {
         } x;
     };
 };
+
+// All regions at one point (the sweep of tauint2, inttau2.f90:51-55,86-96,104-108):
+// signed minimum, minimum |d|, region 0's value, region L's value, the first
+// region containing the point (and its value), and the launch layer
+// (kernelsMod.f90:275-280: innermost containing region).
+template <class T>
+struct SweepOut {
+    T mn, mna, d0, dsL, dsN;
+    int nl, lay;
+};
+template <class T>
+__device__ __forceinline__ SweepOut<T> sweep_regions(const SceneT<T>& sc, V3<T> p, int L) {
+    SweepOut<T> o{(T)INFINITY, (T)INFINITY, (T)0, (T)0, (T)0, -1, 0};
+    T inner = (T)INFINITY;
+    for (int i = 0; i < sc.nregions; ++i) {
+        const T d = eval_region(sc, i, p);
+        o.mn = fmin(o.mn, d);
+        o.mna = fmin(o.mna, fabs(d));
+        if (i == 0) o.d0 = d;
+        if (i == L) o.dsL = d;
+        if (o.nl < 0 && d < (T)0) {
+            o.nl = i;
+            o.dsN = d;
+        }
+        const T a = (d > (T)0) ? (T)999.0 : fabs(d);
+        if (a < inner) {
+            inner = a;
+            o.lay = i;
+        }
+    }
+    return o;
+}
 
 // Single-region evaluations of the crossing path.  They stay inline: an
 // out-of-line function would receive the parameter block by reference and read
@@ -695,109 +729,121 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         }
     }
     // ---- evaluate every region at the current position (the one inlined sweep)
-    if (act == A_SWEEP) {
-        const V3<R> pf = cv<R>(pk.pos);
+    // Within 2 eps of a surface, or resolving a crossing, FP32 transport takes the
+    // decisions (surface reached, crossing step, new region, the kill at a flight's
+    // start) on the FP64 position with the FP64 scene: an FP32 coordinate near 1 cm
+    // is only good to ~1e-7 cm, a tenth of eps, and that noise changed how many
+    // refracted packets the eps rule kills (-0.8% fluence).  Such sweeps are
+    // deferred as A_PRECISE so that they run together, not one lane per warp.
+    if (act == A_SWEEP || act == A_PRECISE) {
         const int L = pk.layer;
-        R mn = (R)INFINITY, mna = (R)INFINITY, inner = (R)INFINITY;
-        R d0 = 0, dsL = 0, dsN = 0;
-        int nl = -1, lay = 0;
-        for (int i = 0; i < N; ++i) {
-            const R d = eval_region(sc, i, pf);
-            mn = fmin(mn, d);
-            mna = fmin(mna, fabs(d));
-            if (i == 0) d0 = d;
-            if (i == L) dsL = d;
-            if (nl < 0 && d < (R)0) {
-                nl = i;
-                dsN = d;
-            }
-            // launch layer (kernelsMod.f90:275-280): innermost containing region
-            const R a = (d > (R)0) ? (R)999.0 : fabs(d);
-            if (a < inner) {
-                inner = a;
-                lay = i;
-            }
+        SweepOut<R> sw;
+        bool precise = false, defer = false;
+        if (sizeof(R) == 4 && act == A_PRECISE) {
+            const SweepOut<double> s64 = sweep_regions(P.sc64, pk.pos, L);
+            sw = SweepOut<R>{(R)s64.mn, (R)s64.mna, (R)s64.d0, (R)s64.dsL, (R)s64.dsN, s64.nl, s64.lay};
+            precise = true;
+        } else {
+            sw = sweep_regions(sc, cv<R>(pk.pos), L);
+            defer = sizeof(R) == 4 && (sw.mna <= (R)2 * eps || f.mode == S_CROSS);
         }
-        c.sdf += N;
-        f.dsdf = mna;
-        const int mode = f.mode;
-        if (mode == S_LAUNCH || mode == S_TOP) {
-            // top of tauint2's outer loop (:51-61).  At launch the same sweep also
-            // gives the layer (the reference evaluates the same point twice).
-            if (mode == S_LAUNCH) {
-                pk.layer = lay;
-                c.sdf += N;
-            }
-            f.steps = 0;
-            // d == eps (reachable on the FP32 coordinate grid) counts as on the
-            // surface, like the reflected packets the reference kills here
-            if (mna <= eps) {
-                pk.tflag = true;
-                act = end_flight(P, pk);
-            } else {
-                act = step_or_skip<R, BATCH, ADJ>(P, pk, f, c, acc);
-            }
-        } else if (mode == S_STEP) {
-            if (mn >= (R)0) {  // outside every region (:92-96)
-                pk.tflag = true;
-                act = end_flight(P, pk);
-            } else if (++f.steps >= P.max_steps) {
-                pk.tflag = true;
-                pk.flags |= STATUS_STEP_CAP;
-                act = end_flight(P, pk);
-            } else if (mna > eps) {
-                act = step_or_skip<R, BATCH, ADJ>(P, pk, f, c, acc);
-            } else if (f.taurun >= f.tau || pk.tflag) {
-                act = end_flight(P, pk);  // (:99-102)
-            } else {
-                // surface reached: count the reference's dstmp sweep (values of this
-                // one, :104-108) and take the crossing step of min|d| + 2 eps
-                c.sdf += N;
-                f.x.oldpos = pk.pos;
-                pk.pos = advance(pk.pos, mna + (R)2 * eps, pk.dir);
-                f.mode = S_CROSS;
-                act = A_SWEEP + 100;  // sweep again at the new position (next iteration)
-            }
-        } else {  // S_CROSS: sweep at the stepped position (:117-184)
-            if (nl < 0) {
-                nl = 0;
-                dsN = d0;
-            }
-            act = A_CROSS;
-            f.mode = S_TOP;
-            if (opt_nidx<R, BATCH>(P, pk.inst, L) != opt_nidx<R, BATCH>(P, pk.inst, nl)) {
-                int which = -1;
-                if (dsL < (R)0 && dsN < (R)0) {
-                    which = (fabs(dsL) <= fabs(dsN)) ? L : nl;
-                } else {
-                    const V3<R> of = cv<R>(f.x.oldpos);
-                    const R tL = eval_region_cold(sc, L, of), tN = eval_region_cold(sc, nl, of);
-                    if (tL < (R)0 && tN < (R)0) {
-                        which = (tL >= tN) ? L : nl;
-                    } else if (dsL >= (R)0 && dsN < (R)0) {
-                        // exactly 0 counts as outside, like the `ds(i) < 0` membership
-                        // test; the `error stop` branch (:155-156) is then reached only by NaN
-                        which = (L == 0) ? L : nl;  // oldlayer = packet%layer, then "== 1" (:150-162)
-                    } else if (dsL >= (R)0 && dsN >= (R)0) {
-                        pk.tflag = true;
-                    } else {
-                        pk.tflag = true;
-                        pk.flags |= STATUS_ERROR_STATE;
-                    }
+        if (defer) {
+            act = A_PRECISE;
+        } else {
+            act = A_SWEEP;
+            const R mn = sw.mn, mna = sw.mna, d0 = sw.d0, dsL = sw.dsL;
+            R dsN = sw.dsN;
+            int nl = sw.nl;
+            const int lay = sw.lay;
+            c.sdf += N;
+            f.dsdf = mna;
+            const int mode = f.mode;
+            if (mode == S_LAUNCH || mode == S_TOP) {
+                // top of tauint2's outer loop (:51-61).  At launch the same sweep also
+                // gives the layer (the reference evaluates the same point twice).
+                if (mode == S_LAUNCH) {
+                    pk.layer = lay;
+                    c.sdf += N;
                 }
-                f.x.which = which;  // the boundary event runs in the A_CROSS phase below
-                f.x.nl = nl;
-            } else {
-                pk.layer = nl;
-                f.x.which = -2;  // same refractive index: continue with the same tau
+                f.steps = 0;
+                // d == eps (reachable on the FP32 coordinate grid) counts as on the
+                // surface, like the reflected packets the reference kills here
+                if (mna <= eps) {
+                    pk.tflag = true;
+                    act = end_flight(P, pk);
+                } else {
+                    act = step_or_skip<R, BATCH, ADJ>(P, pk, f, c, acc);
+                }
+            } else if (mode == S_STEP) {
+                if (mn >= (R)0) {  // outside every region (:92-96)
+                    pk.tflag = true;
+                    act = end_flight(P, pk);
+                } else if (++f.steps >= P.max_steps) {
+                    pk.tflag = true;
+                    pk.flags |= STATUS_STEP_CAP;
+                    act = end_flight(P, pk);
+                } else if (mna > eps) {
+                    act = step_or_skip<R, BATCH, ADJ>(P, pk, f, c, acc);
+                } else if (f.taurun >= f.tau || pk.tflag) {
+                    act = end_flight(P, pk);  // (:99-102)
+                } else {
+                    // surface reached: count the reference's dstmp sweep (values of this
+                    // one, :104-108) and take the crossing step of min|d| + 2 eps
+                    c.sdf += N;
+                    f.x.oldpos = pk.pos;
+                    pk.pos = advance(pk.pos, mna + (R)2 * eps, pk.dir);
+                    f.mode = S_CROSS;
+                    // sweep again at the new position, next round (FP32: in FP64)
+                    act = sizeof(R) == 4 ? A_PRECISE : A_SWEEP + 100;
+                }
+            } else {  // S_CROSS: sweep at the stepped position (:117-184)
+                if (nl < 0) {
+                    nl = 0;
+                    dsN = d0;
+                }
+                act = A_CROSS;
+                f.mode = S_TOP;
+                if (opt_nidx<R, BATCH>(P, pk.inst, L) != opt_nidx<R, BATCH>(P, pk.inst, nl)) {
+                    int which = -1;
+                    if (dsL < (R)0 && dsN < (R)0) {
+                        which = (fabs(dsL) <= fabs(dsN)) ? L : nl;
+                    } else {
+                        R tL, tN;
+                        if (precise) {
+                            tL = (R)eval_region_cold(P.sc64, L, f.x.oldpos);
+                            tN = (R)eval_region_cold(P.sc64, nl, f.x.oldpos);
+                        } else {
+                            const V3<R> of = cv<R>(f.x.oldpos);
+                            tL = eval_region_cold(sc, L, of);
+                            tN = eval_region_cold(sc, nl, of);
+                        }
+                        if (tL < (R)0 && tN < (R)0) {
+                            which = (tL >= tN) ? L : nl;
+                        } else if (dsL >= (R)0 && dsN < (R)0) {
+                            // exactly 0 counts as outside, like the `ds(i) < 0` membership
+                            // test; the `error stop` branch (:155-156) is then reached only by NaN
+                            which = (L == 0) ? L : nl;  // oldlayer = packet%layer, then "== 1" (:150-162)
+                        } else if (dsL >= (R)0 && dsN >= (R)0) {
+                            pk.tflag = true;
+                        } else {
+                            pk.tflag = true;
+                            pk.flags |= STATUS_ERROR_STATE;
+                        }
+                    }
+                    f.x.which = which;  // the boundary event runs in the A_CROSS phase below
+                    f.x.nl = nl;
+                } else {
+                    pk.layer = nl;
+                    f.x.which = -2;  // same refractive index: continue with the same tau
+                }
+                if (pk.tflag) act = end_flight(P, pk);
             }
-            if (pk.tflag) act = end_flight(P, pk);
         }
     }
     if (act == A_SWEEP + 100) act = A_SWEEP;
     // ---- boundary event in FP64: calcNormal + reflect_refract (surfaces.f90:14-40)
     if (act == A_CROSS) {
-        act = A_SWEEP;
+        act = sizeof(R) == 4 ? A_PRECISE : A_SWEEP;  // the next flight starts on the surface
         const int which = f.x.which;
         if (which >= 0) {
             const int L = pk.layer, nl = f.x.nl;
@@ -858,14 +904,15 @@ struct SlotCount {
     static constexpr int n = kBlock * per_thread;
 };
 // Sort groups of the actions a packet can wait in between rounds, in list
-// order: sweep (or a pending crossing), walk, interact, retire/launch.  With the
-// chunk assignment below a warp's first chunk is then mostly sweeps and its
-// second walks, interactions or retirements, so the warps of a CTA run a mix of
-// actions at any time.  (Of the orders measured, this one was fastest on all
-// three benchmark scenes; ordering by pass cost, or pairing cheap with
-// expensive chunks, was slower.)  A_DONE maps to kGroups (not listed).
-constexpr int kGroups = 4;
-__device__ __forceinline__ int act_group(int act) { return (int)((0x4320103u >> (4 * act)) & 0xFu); }
+// order: sweep (or a pending crossing), walk, interact, retire/launch, FP64
+// near-surface sweep.  With the chunk assignment below a warp's first chunk is
+// then mostly sweeps and its second walks, interactions or retirements, so the
+// warps of a CTA run a mix of actions at any time.  (Of the orders measured,
+// sweep-walk-interact-retire was fastest on all three benchmark scenes; ordering
+// by pass cost, or pairing cheap with expensive chunks, was slower.)  A_DONE
+// maps to kGroups (not listed).
+constexpr int kGroups = 5;
+__device__ __forceinline__ int act_group(int act) { return (int)((0x45320103u >> (4 * act)) & 0xFu); }
 
 template <class R, int kSlots = SlotCount<R>::n>
 struct Slots {
@@ -956,7 +1003,7 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
         f.w.ci = (int)sl.u[4 * W][s];
         f.w.cj = (int)sl.u[4 * W + 1][s];
         f.w.ck = (int)sl.u[4 * W + 2][s];
-    } else if (act == A_SWEEP && f.mode == S_CROSS) {
+    } else if ((act == A_SWEEP || act == A_PRECISE) && f.mode == S_CROSS) {
         f.x.oldpos.x = get_r<double>(sl.u, 0, s);
         f.x.oldpos.y = get_r<double>(sl.u, 2, s);
         f.x.oldpos.z = get_r<double>(sl.u, 4, s);
@@ -1007,7 +1054,7 @@ __device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const P
         sl.u[4 * W][s] = (uint32_t)f.w.ci;
         sl.u[4 * W + 1][s] = (uint32_t)f.w.cj;
         sl.u[4 * W + 2][s] = (uint32_t)f.w.ck;
-    } else if (act == A_SWEEP && f.mode == S_CROSS) {
+    } else if ((act == A_SWEEP || act == A_PRECISE) && f.mode == S_CROSS) {
         put_r<double>(sl.u, 0, s, f.x.oldpos.x);
         put_r<double>(sl.u, 2, s, f.x.oldpos.y);
         put_r<double>(sl.u, 4, s, f.x.oldpos.z);

@@ -90,3 +90,11 @@ def test_autotune_keeps_results(cfg):
     assert before.stats["voxel_segments"] == after.stats["voxel_segments"]
     assert np.array_equal(before.bins, after.bins)
     np.testing.assert_allclose(after.jmean, before.jmean, rtol=1e-9, atol=1e-12 * before.jmean.max())
+
+
+def test_fp32_error_matches_fp64_error():
+    """At matched packet counts the FP32 transport's fluence error against a 10x
+    FP64 reference equals the FP64 transport's (its bias is below the noise)."""
+    from signedmcrt_b200.accuracy import error_table
+    t = error_table("box_slab", 200000)
+    assert 0.85 < t["ratio"] < 1.15, t

@@ -399,3 +399,20 @@ def test_camera_bins_shared_and_global(gpu, oracle, nbins):
     assert g.bins.size == (nbins + 1) ** 2
     assert g.bins.sum() > 0
     assert np.array_equal(g.bins, o.bins)
+
+
+@pytest.mark.parametrize("cfg", SCENES)
+def test_fp32_total_path_is_unbiased(gpu, cfg):
+    """The FP32 transport's mean path length per packet equals the FP64
+    transport's within 4 standard errors (8 batches each, independent seeds).
+    Sensitive to ~0.2%: FP32 surface decisions once lost 0.8% here."""
+    st = P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+    n, B = 500000, 8
+    means = {}
+    for prec, base in (("fp32", 100), ("fp64", 200)):
+        with gpu.Transport(arr, st, precision=prec) as tr:
+            means[prec] = np.array([tr.run(n, base + b).jmean.sum() / n for b in range(B)])
+    m32, m64 = means["fp32"], means["fp64"]
+    se = np.sqrt(m32.var(ddof=1) / B + m64.var(ddof=1) / B)
+    assert abs(m32.mean() - m64.mean()) < 4 * se, (m32.mean(), m64.mean(), se)
