@@ -107,6 +107,21 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(power) if power else None}
 
 
+def measured_traffic(config: str, packets: int):
+    """DRAM bytes of one transport launch from the committed ncu record of this
+    workload (profiles/), or None.  The record is a full-size launch; a launch of
+    another size is scaled by packets (the grid's read-in and write-back is fixed,
+    so this is approximate) and says so."""
+    f = ROOT / "profiles" / f"transport_kernel_{config}_dram.json"
+    if not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    t = float(d["dram_bytes_read"] + d["dram_bytes_write"])
+    if packets == d["packets_per_launch"]:
+        return t
+    return {"bytes": t * packets / d["packets_per_launch"], "scaled_from_packets": d["packets_per_launch"]}
+
+
 def algorithmic_work(stats: dict, flat) -> tuple[float, float]:
     """(flop, bytes) of the reference algorithm for the counted events."""
     regions = flat.c.regions
@@ -514,7 +529,7 @@ def main() -> None:
                            l2="flushed between steps (256 MiB write)", precision=args.precision,
                            rng="Philox4x32-10 keyed (seed, packet id)"),
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None,
+                         "frac": achieved_gbs / pk["hbm_gbs"], "traffic": measured_traffic(args.config, per_gpu),
                          "peak_source": pk["source"],
                          "bytes_per_packet": nbytes / stats["packets"],
                          "kernel_ms": kmean,
