@@ -904,15 +904,15 @@ struct SlotCount {
     static constexpr int n = kBlock * per_thread;
 };
 // Sort groups of the actions a packet can wait in between rounds, in list
-// order: sweep (or a pending crossing), walk, interact, retire/launch, FP64
-// near-surface sweep.  With the chunk assignment below a warp's first chunk is
-// then mostly sweeps and its second walks, interactions or retirements, so the
-// warps of a CTA run a mix of actions at any time.  (Of the orders measured,
-// sweep-walk-interact-retire was fastest on all three benchmark scenes; ordering
-// by pass cost, or pairing cheap with expensive chunks, was slower.)  A_DONE
-// maps to kGroups (not listed).
+// order: FP64 near-surface sweep, sweep (or a pending crossing), walk, interact,
+// retire/launch.  With the chunk assignment below the costly FP64 chunks are some
+// warps' first chunk, and a warp's two chunks come from different parts of the
+// list, so the warps of a CTA run a mix of actions at any time.  (Of the orders
+// measured this one was fastest on all three benchmark scenes; ordering by pass
+// cost, or pairing cheap with expensive chunks, was slower.)  A_DONE maps to
+// kGroups (not listed).
 constexpr int kGroups = 5;
-__device__ __forceinline__ int act_group(int act) { return (int)((0x45320103u >> (4 * act)) & 0xFu); }
+__device__ __forceinline__ int act_group(int act) { return (int)((0x05431214u >> (4 * act)) & 0xFu); }
 
 template <class R, int kSlots = SlotCount<R>::n>
 struct Slots {
