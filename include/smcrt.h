@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define SMCRT_ABI_VERSION 1
+#define SMCRT_ABI_VERSION 2
 
 /* ---- status codes -------------------------------------------------------- */
 enum smcrt_status {
@@ -75,11 +75,28 @@ enum smcrt_csg_op {
     SMCRT_OP_INTERSECTION = 4
 };
 
+/* SDF modifiers wrapping a primitive (src/sdfs/sdfModifiers.f90:273-375).  The
+ * modifier has no transform of its own; the primitive keeps its transform.
+ * (displacement takes a user function and repeat is not implemented in the
+ * reference, so neither exists here.) */
+enum smcrt_modifier {
+    SMCRT_MOD_NONE = 0,
+    SMCRT_MOD_ONION = 1,      /* [thickness]: |d| - t                 eval_onion :307-317 */
+    SMCRT_MOD_REVOLUTION = 2, /* [o]: prim at (|(x,z)| - o, y, 0)      eval_revolution :290-305 */
+    SMCRT_MOD_EXTRUDE = 3,    /* [h]: extrusion of the xy profile      eval_extrude :273-288 */
+    SMCRT_MOD_ELONGATE = 4,   /* [sx, sy, sz]                          eval_elongate :319-335 */
+    SMCRT_MOD_TWIST = 5,      /* [k]: rotation by k z about z          eval_twist :337-355 */
+    SMCRT_MOD_BEND = 6        /* [k]: rotation by k x about z          eval_bend :357-375 */
+};
+
 typedef struct smcrt_prim {
     int32_t kind;          /* smcrt_prim_kind */
-    int32_t reserved;
+    int32_t nmods;         /* modifiers applied to this primitive, 0..2 */
     double transform[4][3];
     double params[8];
+    int32_t mods[2];       /* smcrt_modifier, innermost first: onion(revolution(egg)) =
+                              {REVOLUTION, ONION} */
+    double mod_params[2][3];
 } smcrt_prim;
 
 /* One entry of the reference's sdf array: a single primitive (nprims == 1) or a

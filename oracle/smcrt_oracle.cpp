@@ -56,6 +56,9 @@ struct Prim {
     int kind;
     R m[4][3];
     R p[8];
+    int nmods;
+    int mod[2];
+    R mp[2][3];
 };
 template <class R>
 struct Region {
@@ -79,6 +82,11 @@ Scene<R> make_scene(const smcrt_scene* s) {
         for (int a = 0; a < 4; ++a)
             for (int b = 0; b < 3; ++b) p.m[a][b] = (R)s->prims[i].transform[a][b];
         for (int a = 0; a < 8; ++a) p.p[a] = (R)s->prims[i].params[a];
+        p.nmods = s->prims[i].nmods;
+        for (int j = 0; j < 2; ++j) {
+            p.mod[j] = s->prims[i].mods[j];
+            for (int a = 0; a < 3; ++a) p.mp[j][a] = (R)s->prims[i].mod_params[j][a];
+        }
         out.prims.push_back(p);
     }
     for (int i = 0; i < s->nregions; ++i) {
@@ -104,8 +112,12 @@ Scene<R> make_scene(const smcrt_scene* s) {
 
 int validate_scene(const smcrt_scene* s) {
     if (!s || s->nregions <= 0 || s->nprims <= 0 || !s->regions || !s->prims) return 1;
-    for (int i = 0; i < s->nprims; ++i)
+    for (int i = 0; i < s->nprims; ++i) {
         if (s->prims[i].kind < SMCRT_SPHERE || s->prims[i].kind > SMCRT_PLANE) return 1;
+        if (s->prims[i].nmods < 0 || s->prims[i].nmods > 2) return 1;
+        for (int j = 0; j < s->prims[i].nmods; ++j)
+            if (s->prims[i].mods[j] < SMCRT_MOD_ONION || s->prims[i].mods[j] > SMCRT_MOD_BEND) return 1;
+    }
     for (int i = 0; i < s->nregions; ++i) {
         const smcrt_region& r = s->regions[i];
         if (r.nprims <= 0 || r.first_prim < 0 || r.first_prim + r.nprims > s->nprims) return 1;
@@ -126,7 +138,7 @@ inline V3<R> xform(const R m[4][3], V3<R> a) {
 
 // Primitive SDFs, src/sdfs/sdfs.f90:494-735
 template <class R>
-R eval_prim(const Prim<R>& pr, V3<R> pos) {
+R eval_prim_base(const Prim<R>& pr, V3<R> pos) {
     V3<R> p = xform(pr.m, pos);
     const R* q = pr.p;
     const R zero = 0, one = 1, half = (R)0.5;
@@ -202,6 +214,51 @@ R eval_prim(const Prim<R>& pr, V3<R> pos) {
             return dot(p, V3<R>{q[0], q[1], q[2]});
     }
     return zero;
+}
+
+// Modifiers, src/sdfs/sdfModifiers.f90:273-375: eval_revolution (:290-305),
+// eval_elongate (:319-335), eval_twist (:337-355), eval_bend (:357-375) change the
+// point the wrapped SDF is evaluated at; eval_onion (:307-317), eval_extrude
+// (:273-288) and eval_elongate change its value.  The wrapped primitive applies
+// its own transform; a modifier has none.
+template <class R>
+V3<R> mod_point(int kind, const R* q, V3<R> p) {
+    const R zero = 0;
+    if (kind == SMCRT_MOD_REVOLUTION) return V3<R>{length(V3<R>{p.x, p.z, zero}) - q[0], p.y, zero};
+    if (kind == SMCRT_MOD_ELONGATE)
+        return V3<R>{std::max(std::fabs(p.x) - q[0], zero), std::max(std::fabs(p.y) - q[1], zero),
+                     std::max(std::fabs(p.z) - q[2], zero)};
+    if (kind == SMCRT_MOD_TWIST || kind == SMCRT_MOD_BEND) {
+        const R a = q[0] * (kind == SMCRT_MOD_TWIST ? p.z : p.x);
+        const R c = std::cos(a), s = std::sin(a);
+        return V3<R>{c * p.x - s * p.y, s * p.x + c * p.y, p.z};
+    }
+    return p;
+}
+template <class R>
+R mod_value(int kind, const R* q, R d, V3<R> p) {
+    const R zero = 0;
+    if (kind == SMCRT_MOD_ONION) return std::fabs(d) - q[0];
+    if (kind == SMCRT_MOD_EXTRUDE) {
+        const V3<R> w{d, std::fabs(p.z) - q[0], zero};
+        return std::min(std::max(w.x, w.y), zero) + length(vmax(w, zero));
+    }
+    if (kind == SMCRT_MOD_ELONGATE) {
+        const V3<R> e = vabs(p) - V3<R>{q[0], q[1], q[2]};
+        return d + std::min(std::max(e.x, std::max(e.y, e.z)), zero);
+    }
+    return d;
+}
+// onion(revolution(egg)): the outer modifier's point map first, the inner's value
+// map first -- the nested evaluate calls of the reference.
+template <class R>
+R eval_prim(const Prim<R>& pr, V3<R> pos) {
+    if (pr.nmods == 0) return eval_prim_base(pr, pos);
+    const V3<R> p1 = pr.nmods == 2 ? mod_point(pr.mod[1], pr.mp[1], pos) : pos;
+    const V3<R> p2 = mod_point(pr.mod[0], pr.mp[0], p1);
+    R d = mod_value(pr.mod[0], pr.mp[0], eval_prim_base(pr, p2), p1);
+    if (pr.nmods == 2) d = mod_value(pr.mod[1], pr.mp[1], d, pos);
+    return d;
 }
 
 // eval_model (src/sdfs/sdf_base.f90:145-160) with the CSG ops of

@@ -8,7 +8,7 @@ import ctypes as C
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # status
 OK, ERR_ARG, ERR_SCENE, ERR_CUDA, ERR_DEVICE, ERR_TIMEOUT, ERR_NO_DEVICE = range(7)
@@ -30,8 +30,9 @@ D3 = C.c_double * 3
 
 
 class Prim(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32),
-                ("transform", (C.c_double * 3) * 4), ("params", C.c_double * 8)]
+    _fields_ = [("kind", C.c_int32), ("nmods", C.c_int32),
+                ("transform", (C.c_double * 3) * 4), ("params", C.c_double * 8),
+                ("mods", C.c_int32 * 2), ("mod_params", (C.c_double * 3) * 2)]
 
 
 class Region(C.Structure):
@@ -117,6 +118,9 @@ def u32ptr(a: np.ndarray):
 def i32ptr(a: np.ndarray):
     assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+MOD_NONE, MOD_ONION, MOD_REVOLUTION, MOD_EXTRUDE, MOD_ELONGATE, MOD_TWIST, MOD_BEND = range(7)
 
 
 class RegionOptics(C.Structure):

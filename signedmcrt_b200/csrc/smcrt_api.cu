@@ -40,9 +40,16 @@ int validate_scene(const smcrt_scene* s) {
     if (s->nregions > kMaxRegions || s->nprims > kMaxPrims)
         return fail(SMCRT_ERR_SCENE, "scene: at most " + std::to_string(kMaxRegions) + " regions and " +
                                          std::to_string(kMaxPrims) + " primitives");
-    for (int i = 0; i < s->nprims; ++i)
-        if (s->prims[i].kind < SMCRT_SPHERE || s->prims[i].kind > SMCRT_PLANE)
+    for (int i = 0; i < s->nprims; ++i) {
+        const smcrt_prim& pr = s->prims[i];
+        if (pr.kind < SMCRT_SPHERE || pr.kind > SMCRT_PLANE)
             return fail(SMCRT_ERR_SCENE, "scene: unknown primitive kind at " + std::to_string(i));
+        if (pr.nmods < 0 || pr.nmods > 2)
+            return fail(SMCRT_ERR_SCENE, "scene: primitive " + std::to_string(i) + " needs 0..2 modifiers");
+        for (int j = 0; j < pr.nmods; ++j)
+            if (pr.mods[j] < SMCRT_MOD_ONION || pr.mods[j] > SMCRT_MOD_BEND)
+                return fail(SMCRT_ERR_SCENE, "scene: unknown modifier on primitive " + std::to_string(i));
+    }
     for (int i = 0; i < s->nregions; ++i) {
         const smcrt_region& r = s->regions[i];
         if (r.nprims <= 0 || r.first_prim < 0 || r.first_prim + r.nprims > s->nprims)

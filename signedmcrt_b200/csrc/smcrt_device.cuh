@@ -50,7 +50,9 @@ struct DPrim {
     R m[12];  // row-vector affine, m[3*i+j] = M[i][j]
     R q[8];
     int kind;
-    int pad;
+    int nmods;   // modifiers, innermost first
+    int mod[2];
+    R mp[2][3];
 };
 template <class R>
 struct DRegion {
@@ -70,6 +72,7 @@ struct InstOptics {
 template <class R>
 struct SceneT {
     int nregions, nprims;
+    int has_mods, pad;  // some primitive carries modifiers
     DPrim<R> prim[kMaxPrims];
     DRegion<R> region[kMaxRegions];
 };
@@ -86,7 +89,7 @@ __device__ __forceinline__ V3<R> xform(const R* m, V3<R> a) {
 
 // Primitive SDFs, src/sdfs/sdfs.f90:494-735
 template <class R>
-__device__ __forceinline__ R eval_prim(const DPrim<R>& pr, V3<R> pos) {
+__device__ __forceinline__ R eval_prim_base(const DPrim<R>& pr, V3<R> pos) {
     const V3<R> p = xform(pr.m, pos);
     const R* q = pr.q;
     const R zero = 0, one = 1, half = (R)0.5;
@@ -163,13 +166,70 @@ __device__ __forceinline__ R eval_prim(const DPrim<R>& pr, V3<R> pos) {
     return zero;
 }
 
-// eval_model (src/sdfs/sdf_base.f90:145-160), CSG ops src/sdfs/sdfModifiers.f90:412-475
+// Modifiers (src/sdfs/sdfModifiers.f90:273-375): the point the wrapped SDF is
+// evaluated at, and the value the modifier returns from the wrapped SDF's value.
 template <class R>
+__device__ __forceinline__ V3<R> mod_point(int kind, const R* q, V3<R> p) {
+    const R zero = 0;
+    switch (kind) {
+        case SMCRT_MOD_REVOLUTION:  // (|(x, z)| - o, y, 0)
+            return V3<R>{sqrt(p.x * p.x + p.z * p.z + zero * zero) - q[0], p.y, zero};
+        case SMCRT_MOD_ELONGATE:  // max(|p| - size, 0)
+            return V3<R>{fmax(fabs(p.x) - q[0], zero), fmax(fabs(p.y) - q[1], zero), fmax(fabs(p.z) - q[2], zero)};
+        case SMCRT_MOD_TWIST: {  // rotation by k z about z
+            R s, c;
+            sincos_r(q[0] * p.z, &s, &c);
+            return V3<R>{c * p.x - s * p.y, s * p.x + c * p.y, p.z};
+        }
+        case SMCRT_MOD_BEND: {  // rotation by k x about z
+            R s, c;
+            sincos_r(q[0] * p.x, &s, &c);
+            return V3<R>{c * p.x - s * p.y, s * p.x + c * p.y, p.z};
+        }
+        default:  // onion, extrude: the wrapped SDF sees the point itself
+            return p;
+    }
+}
+template <class R>
+__device__ __forceinline__ R mod_value(int kind, const R* q, R d, V3<R> p) {
+    const R zero = 0;
+    switch (kind) {
+        case SMCRT_MOD_ONION:
+            return fabs(d) - q[0];
+        case SMCRT_MOD_EXTRUDE: {  // w = (d, |z| - h, 0)
+            const R wy = fabs(p.z) - q[0];
+            const R mx = fmax(d, zero), my = fmax(wy, zero);
+            return fmin(fmax(d, wy), zero) + sqrt(mx * mx + my * my + zero * zero);
+        }
+        case SMCRT_MOD_ELONGATE: {
+            const R qx = fabs(p.x) - q[0], qy = fabs(p.y) - q[1], qz = fabs(p.z) - q[2];
+            return d + fmin(fmax(qx, fmax(qy, qz)), zero);
+        }
+        default:
+            return d;
+    }
+}
+
+// A primitive with its modifiers: points map outermost modifier first, values
+// innermost first, as the nested evaluate calls of the reference do.  MODS =
+// false compiles the primitive alone, for scenes without modifiers.
+template <class R, bool MODS = true>
+__device__ __forceinline__ R eval_prim(const DPrim<R>& pr, V3<R> pos) {
+    if (!MODS || pr.nmods == 0) return eval_prim_base(pr, pos);
+    const V3<R> p1 = pr.nmods == 2 ? mod_point(pr.mod[1], pr.mp[1], pos) : pos;
+    const V3<R> p2 = mod_point(pr.mod[0], pr.mp[0], p1);
+    R d = mod_value(pr.mod[0], pr.mp[0], eval_prim_base(pr, p2), p1);
+    if (pr.nmods == 2) d = mod_value(pr.mod[1], pr.mp[1], d, pos);
+    return d;
+}
+
+// eval_model (src/sdfs/sdf_base.f90:145-160), CSG ops src/sdfs/sdfModifiers.f90:412-475
+template <class R, bool MODS = true>
 __device__ __forceinline__ R eval_region(const SceneT<R>& sc, int r, V3<R> pos) {
     const DRegion<R>& g = sc.region[r];
-    R d = eval_prim(sc.prim[g.first], pos);
+    R d = eval_prim<R, MODS>(sc.prim[g.first], pos);
     for (int i = 1; i < g.n; ++i) {
-        R d2 = eval_prim(sc.prim[g.first + i], pos);
+        R d2 = eval_prim<R, MODS>(sc.prim[g.first + i], pos);
         switch (g.op) {
             case SMCRT_OP_UNION: d = fmin(d, d2); break;
             case SMCRT_OP_SMOOTH_UNION: {
@@ -185,10 +245,13 @@ __device__ __forceinline__ R eval_region(const SceneT<R>& sc, int r, V3<R> pos) 
 }
 
 // calcNormal, src/sdfs/sdf_base.f90:165-189 (always double)
+template <bool MODS = true>
 __device__ __forceinline__ V3<double> calc_normal(const SceneT<double>& sc, int r, V3<double> p, double h) {
     const V3<double> xyy{1, -1, -1}, yyx{-1, -1, 1}, yxy{-1, 1, -1}, xxx{1, 1, 1};
-    V3<double> n = xyy * eval_region(sc, r, p + xyy * h) + yyx * eval_region(sc, r, p + yyx * h) +
-                   yxy * eval_region(sc, r, p + yxy * h) + xxx * eval_region(sc, r, p + xxx * h);
+    V3<double> n = xyy * eval_region<double, MODS>(sc, r, p + xyy * h) +
+                   yyx * eval_region<double, MODS>(sc, r, p + yyx * h) +
+                   yxy * eval_region<double, MODS>(sc, r, p + yxy * h) +
+                   xxx * eval_region<double, MODS>(sc, r, p + xxx * h);
     double t = len3(n);
     return V3<double>{n.x / t, n.y / t, n.z / t};
 }

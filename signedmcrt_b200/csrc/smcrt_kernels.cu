@@ -14,10 +14,12 @@ namespace smcrt {
 
 // Dynamic shared memory of a launch: the CTA's packet slots, then the
 // privatized detector bins.  The kernel needs more than the default 48 KiB
-// opt-in limit, set once per kernel.
-template <bool REPLAY>
+// opt-in limit, set once per kernel.  Scenes whose primitives carry no
+// modifiers run the instantiation compiled without the modifier code
+// (MODS = false); replays always run the general one.
+template <bool REPLAY, bool MODS = true>
 static cudaError_t allow_smem() {
-    static const cudaError_t e = cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, REPLAY>,
+    static const cudaError_t e = cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, REPLAY, false, false, MODS>,
                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                       (int)(slots_bytes<SMCRT_R>() + sizeof(unsigned) * kMaxSharedBins));
     return e;
@@ -27,10 +29,12 @@ cudaError_t SMCRT_CAT(launch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, cons
                                                    int block, cudaStream_t s) {
     if (block != kBlock) return cudaErrorInvalidConfiguration;
     const size_t smem = slots_bytes<SMCRT_R>() + sizeof(unsigned) * (size_t)P.sbins;
-    cudaError_t e = replay ? allow_smem<true>() : allow_smem<false>();
+    const bool mods = P.sc.has_mods != 0;
+    cudaError_t e = replay ? allow_smem<true>() : mods ? allow_smem<false>() : allow_smem<false, false>();
     if (e != cudaSuccess) return e;
     if (replay) transport_kernel<SMCRT_R, SMCRT_K, true><<<blocks, kBlock, smem, s>>>(P, B);
-    else transport_kernel<SMCRT_R, SMCRT_K, false><<<blocks, kBlock, smem, s>>>(P, B);
+    else if (mods) transport_kernel<SMCRT_R, SMCRT_K, false><<<blocks, kBlock, smem, s>>>(P, B);
+    else transport_kernel<SMCRT_R, SMCRT_K, false, false, false, false><<<blocks, kBlock, smem, s>>>(P, B);
     return cudaGetLastError();
 }
 
@@ -45,8 +49,16 @@ cudaError_t SMCRT_CAT(launch_batch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P
     static const cudaError_t attr = cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, false, true>,
                                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                          (int)slots_bytes<SMCRT_R>());
+    static const cudaError_t attr0 =
+        cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, false, true, false, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slots_bytes<SMCRT_R>());
     if (attr != cudaSuccess) return attr;
-    transport_kernel<SMCRT_R, SMCRT_K, false, true><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
+    if (attr0 != cudaSuccess) return attr0;
+    if (P.sc.has_mods)
+        transport_kernel<SMCRT_R, SMCRT_K, false, true><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
+    else
+        transport_kernel<SMCRT_R, SMCRT_K, false, true, false, false>
+            <<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
     return cudaGetLastError();
 #endif
 }
@@ -62,9 +74,16 @@ cudaError_t SMCRT_CAT(launch_adjoint, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>&
     static const cudaError_t attr = cudaFuncSetAttribute(transport_kernel<SMCRT_R, 0, false, false, true>,
                                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                          (int)slots_bytes<SMCRT_R>());
+    static const cudaError_t attr0 =
+        cudaFuncSetAttribute(transport_kernel<SMCRT_R, 0, false, false, true, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slots_bytes<SMCRT_R>());
     if (attr != cudaSuccess) return attr;
+    if (attr0 != cudaSuccess) return attr0;
     if (blocks == 0) return cudaSuccess;
-    transport_kernel<SMCRT_R, 0, false, false, true><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
+    if (P.sc.has_mods)
+        transport_kernel<SMCRT_R, 0, false, false, true><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
+    else
+        transport_kernel<SMCRT_R, 0, false, false, true, false><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
     return cudaGetLastError();
 #endif
 }

@@ -12,11 +12,18 @@ void fill_scene(SceneT<R>& d, const smcrt_scene* s) {
     std::memset(&d, 0, sizeof(d));
     d.nregions = s->nregions;
     d.nprims = s->nprims;
+    d.has_mods = 0;
+    for (int i = 0; i < s->nprims; ++i) d.has_mods |= s->prims[i].nmods > 0;
     for (int i = 0; i < s->nprims; ++i) {
         for (int a = 0; a < 4; ++a)
             for (int b = 0; b < 3; ++b) d.prim[i].m[3 * a + b] = (R)s->prims[i].transform[a][b];
         for (int a = 0; a < 8; ++a) d.prim[i].q[a] = (R)s->prims[i].params[a];
         d.prim[i].kind = s->prims[i].kind;
+        d.prim[i].nmods = s->prims[i].nmods;
+        for (int j = 0; j < 2; ++j) {
+            d.prim[i].mod[j] = s->prims[i].mods[j];
+            for (int a = 0; a < 3; ++a) d.prim[i].mp[j][a] = (R)s->prims[i].mod_params[j][a];
+        }
     }
     for (int i = 0; i < s->nregions; ++i) {
         const smcrt_region& g = s->regions[i];

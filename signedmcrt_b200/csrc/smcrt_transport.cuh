@@ -313,12 +313,12 @@ struct SweepOut {
     T mn, mna, d0, dsL, dsN;
     int nl, lay;
 };
-template <class T>
+template <class T, bool MODS = true>
 __device__ __forceinline__ SweepOut<T> sweep_regions(const SceneT<T>& sc, V3<T> p, int L) {
     SweepOut<T> o{(T)INFINITY, (T)INFINITY, (T)0, (T)0, (T)0, -1, 0};
     T inner = (T)INFINITY;
     for (int i = 0; i < sc.nregions; ++i) {
-        const T d = eval_region(sc, i, p);
+        const T d = eval_region<T, MODS>(sc, i, p);
         o.mn = fmin(o.mn, d);
         o.mna = fmin(o.mna, fabs(d));
         if (i == 0) o.d0 = d;
@@ -339,12 +339,13 @@ __device__ __forceinline__ SweepOut<T> sweep_regions(const SceneT<T>& sc, V3<T> 
 // Single-region evaluations of the crossing path.  They stay inline: an
 // out-of-line function would receive the parameter block by reference and read
 // it through generic loads instead of the constant bank.
-template <class R>
+template <class R, bool MODS>
 __device__ __forceinline__ R eval_region_cold(const SceneT<R>& sc, int r, V3<R> p) {
-    return eval_region(sc, r, p);
+    return eval_region<R, MODS>(sc, r, p);
 }
+template <bool MODS>
 __device__ __forceinline__ V3<double> calc_normal_cold(const SceneT<double>& sc, int r, V3<double> p, double h) {
-    return calc_normal(sc, r, p, h);
+    return calc_normal<MODS>(sc, r, p, h);
 }
 
 // Step start in grid coordinates (the position does not move during a walk).
@@ -550,7 +551,7 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
 // SMCRT_WALK_SEGMENTS voxel segments.  A packet can pass through several
 // actions in one pass (retire -> launch -> sweep -> walk, interact -> sweep ->
 // walk, sweep -> cross).  `c` counts this thread's events since its last flush.
-template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ>
+template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ, bool MODS>
 __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers& B, Pk<R>& pk, Flight<R>& f,
                                                Stream<R, REPLAY>& rng, Cnt& c, int& act, unsigned long long* s_cnt,
                                                double* s_mom, unsigned* s_bins, float* acc) {
@@ -740,11 +741,11 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         SweepOut<R> sw;
         bool precise = false, defer = false;
         if (sizeof(R) == 4 && act == A_PRECISE) {
-            const SweepOut<double> s64 = sweep_regions(P.sc64, pk.pos, L);
+            const SweepOut<double> s64 = sweep_regions<double, MODS>(P.sc64, pk.pos, L);
             sw = SweepOut<R>{(R)s64.mn, (R)s64.mna, (R)s64.d0, (R)s64.dsL, (R)s64.dsN, s64.nl, s64.lay};
             precise = true;
         } else {
-            sw = sweep_regions(sc, cv<R>(pk.pos), L);
+            sw = sweep_regions<R, MODS>(sc, cv<R>(pk.pos), L);
             defer = sizeof(R) == 4 && (sw.mna <= (R)2 * eps || f.mode == S_CROSS);
         }
         if (defer) {
@@ -810,12 +811,12 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                     } else {
                         R tL, tN;
                         if (precise) {
-                            tL = (R)eval_region_cold(P.sc64, L, f.x.oldpos);
-                            tN = (R)eval_region_cold(P.sc64, nl, f.x.oldpos);
+                            tL = (R)eval_region_cold<double, MODS>(P.sc64, L, f.x.oldpos);
+                            tN = (R)eval_region_cold<double, MODS>(P.sc64, nl, f.x.oldpos);
                         } else {
                             const V3<R> of = cv<R>(f.x.oldpos);
-                            tL = eval_region_cold(sc, L, of);
-                            tN = eval_region_cold(sc, nl, of);
+                            tL = eval_region_cold<R, MODS>(sc, L, of);
+                            tN = eval_region_cold<R, MODS>(sc, nl, of);
                         }
                         if (tL < (R)0 && tN < (R)0) {
                             which = (tL >= tN) ? L : nl;
@@ -849,7 +850,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             const int L = pk.layer, nl = f.x.nl;
             ++c.fres;
             c.sdf += 4;
-            const V3<double> Nn = calc_normal_cold(P.sc64, which, pk.pos, P.normal_h);
+            const V3<double> Nn = calc_normal_cold<MODS>(P.sc64, which, pk.pos, P.normal_h);
             V3<double> I{(double)pk.dir.x, (double)pk.dir.y, (double)pk.dir.z};
             const double m1 = opt_nidx64<R, BATCH>(P, pk.inst, L), m2 = opt_nidx64<R, BATCH>(P, pk.inst, nl);
             const double Rf = fresnel(I, Nn, m1, m2);
@@ -1079,7 +1080,9 @@ __host__ __device__ constexpr size_t slots_bytes() {
 // works on 32 packets that start the pass with the same action, whatever mix of
 // actions the CTA's packets are in; rare actions (boundary events, retire and
 // launch) are gathered across the CTA instead of stalling 31 idle lanes.
-template <class R, int KERNEL, bool REPLAY, bool BATCH = false, bool ADJ = false>
+// MODS = false compiles every distance evaluation without the modifier code,
+// for scenes whose primitives carry no modifiers.
+template <class R, int KERNEL, bool REPLAY, bool BATCH = false, bool ADJ = false, bool MODS = true>
 __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
                                                                              const Buffers B) {
     constexpr int Q = SlotCount<R>::per_thread;
@@ -1183,7 +1186,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         for (int i = t; i < total; i += kBlock) {
             const int s = s_list[i];
             int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc);
+            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc);
             store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
         }
     }

@@ -46,6 +46,19 @@ def setup_omg_sdf() -> list:
     return [S.model(c, S.smooth_union, 0.09), S.box((2.0, 2.0, 2.0), S.mono(0.0, 0.0, 0.0, 1.0), 2)]
 
 
+def setup_egg() -> list:
+    """setupGeometry.f90:10-61 ("test_egg"): a sphere yolk (r 1.5), the albumen as a
+    revolved egg and the shell as the onion of a revolved egg, in a 40 cm box."""
+    r1 = 3.0
+    r2 = 3.0 * math.sqrt(2.0 - math.sqrt(2.0))
+    h = r2
+    shell = S.onion(S.revolution(S.egg(r1, r2, h, S.mono(100.0, 10.0, 0.0, 1.37), 2), 0.2), 0.2)
+    albumen = S.revolution(S.egg(r1 - 0.2, r2, h, S.mono(1.0, 0.0, 0.0, 1.37), 3), 0.2)
+    yolk = S.sphere(1.5, S.mono(10.0, 1.0, 0.9, 1.37), 1)
+    bbox = S.box((20.001, 20.001, 20.001), S.mono(0.0, 0.0, 0.0, 1.0), 4)
+    return [yolk, albumen, shell, bbox]
+
+
 def setup_sphere_scene(num_spheres: int, seed: int) -> list:
     """setupGeometry.f90:62-106: random non-scattering spheres in a 2 cm box.  The
     reference draws radii/positions from the gfortran stream; here from a seeded
@@ -143,9 +156,11 @@ def setup_simulation(st: Settings) -> list:
         return sphere_water()
     if name == "layered_vessels":
         return layered_vessels()
-    if name in ("logo", "vessels", "test_egg"):
+    if name == "test_egg":
+        return setup_egg()
+    if name in ("logo", "vessels"):
         raise ConfigError(f"preset '{name}' needs geometry this transport does not model "
-                          "(svg include, external vessel files, or revolution/onion modifiers)")
+                          "(an svg include or external vessel files)")
     raise ConfigError("no such routine")  # setup.f90:51
 
 

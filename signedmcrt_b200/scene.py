@@ -125,6 +125,45 @@ class Sdf:
     opt: Mono
     layer: int
     transform: np.ndarray = field(default_factory=identity)
+    mods: tuple = ()  # ((modifier kind, params), ...), innermost first
+
+
+# ---------------------------------------------------------------- modifiers (sdfModifiers.f90:114-375)
+# Each wraps an Sdf (a primitive, possibly already modified) and keeps its optics
+# and layer, like the *_init functions; the modifier has no transform of its own.
+MAX_MODIFIERS = 2
+
+
+def _wrap(prim: Sdf, kind: int, params) -> Sdf:
+    if len(prim.mods) >= MAX_MODIFIERS:
+        raise ValueError(f"at most {MAX_MODIFIERS} modifiers per primitive")
+    return Sdf(prim.kind, prim.params, prim.opt, prim.layer, prim.transform,
+               prim.mods + ((kind, tuple(float(x) for x in params)),))
+
+
+def onion(prim: Sdf, thickness: float) -> Sdf:  # onion_init, eval_onion
+    return _wrap(prim, abi.MOD_ONION, (thickness,))
+
+
+def revolution(prim: Sdf, o: float) -> Sdf:  # revolution_init, eval_revolution
+    return _wrap(prim, abi.MOD_REVOLUTION, (o,))
+
+
+def extrude(prim: Sdf, h: float) -> Sdf:  # extrude_init, eval_extrude
+    return _wrap(prim, abi.MOD_EXTRUDE, (h,))
+
+
+def elongate(prim: Sdf, size) -> Sdf:  # elongate_init, eval_elongate
+    return _wrap(prim, abi.MOD_ELONGATE, tuple(size))
+
+
+def twist(prim: Sdf, k: float) -> Sdf:
+    """twist_init takes k as a default (single precision) real: k is rounded to FP32."""
+    return _wrap(prim, abi.MOD_TWIST, (float(np.float32(k)),))
+
+
+def bend(prim: Sdf, k: float) -> Sdf:  # bend_init, eval_bend
+    return _wrap(prim, abi.MOD_BEND, (k,))
 
 
 def _t(transform) -> np.ndarray:
@@ -222,6 +261,11 @@ class FlatScene:
                         p.transform[i][j] = float(m[i, j])
                 for i, v in enumerate(s.params):
                     p.params[i] = v
+                p.nmods = len(s.mods)
+                for j, (mk, mp) in enumerate(s.mods):
+                    p.mods[j] = mk
+                    for i, v in enumerate(mp):
+                        p.mod_params[j][i] = v
                 prims.append(p)
             r = abi.Region()
             r.first_prim = first

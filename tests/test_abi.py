@@ -53,7 +53,7 @@ def test_no_device_is_an_error_not_a_crash():
 
 
 STRUCTS = {
-    "smcrt_prim": (abi.Prim, ["kind", "transform", "params"]),
+    "smcrt_prim": (abi.Prim, ["kind", "nmods", "transform", "params", "mods", "mod_params"]),
     "smcrt_region": (abi.Region, ["first_prim", "nprims", "op", "layer_id", "k", "mus", "mua", "hgg", "n"]),
     "smcrt_scene": (abi.Scene, ["nregions", "nprims", "regions", "prims"]),
     "smcrt_grid": (abi.Grid, ["nxg", "nyg", "nzg", "xmax", "ymax", "zmax"]),

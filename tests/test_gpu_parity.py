@@ -416,3 +416,40 @@ def test_fp32_total_path_is_unbiased(gpu, cfg):
     m32, m64 = means["fp32"], means["fp64"]
     se = np.sqrt(m32.var(ddof=1) / B + m64.var(ddof=1) / B)
     assert abs(m32.mean() - m64.mean()) < 4 * se, (m32.mean(), m64.mean(), se)
+
+
+def modifier_scene():
+    o = OPT0
+    box = S.box((1.0, 0.4, 2.0), o, 1)
+    sph = S.sphere(0.8, o, 1)
+    egg = S.egg(3.0, 2.3, 2.3, o, 1)
+    return S.FlatScene([S.onion(sph, 0.1), S.revolution(S.sphere(0.3, o, 1), 1.1), S.extrude(sph, 0.3),
+                        S.elongate(S.sphere(0.3, o, 1), (0.7, 0.2, 0.0)), S.twist(box, 0.7), S.bend(box, 0.9),
+                        S.onion(S.revolution(egg, 0.2), 0.2)])
+
+
+def test_modified_primitives_on_device(gpu, oracle):
+    flat = modifier_scene()
+    pts = np.random.default_rng(11).uniform(-3, 3, (4000, 3))
+    want = oracle.eval_sdf(flat, pts, "fp64")
+    got64 = gpu.eval_sdf(flat, pts, "fp64")
+    np.testing.assert_allclose(got64, want, rtol=1e-12, atol=1e-12)
+    got32 = gpu.eval_sdf(flat, pts, "fp32")
+    assert np.all(np.abs(got32 - want) <= TOL32 * np.maximum(1.0, np.abs(want)))
+
+
+def test_egg_preset_fp64_transport_matches_oracle(gpu, oracle):
+    """The reference's test_egg scene (onion and revolution modifiers): FP64 event
+    counters identical to the oracle's."""
+    st = P.benchmark_settings("box_slab")
+    st.grid.nxg = st.grid.nyg = st.grid.nzg = 40
+    st.grid.xmax = st.grid.ymax = st.grid.zmax = 4.0
+    st.source.position = (0.0, 0.0, 3.9)
+    arr = P.setup_egg()
+    with gpu.Transport(arr, st, precision="fp64") as tr:
+        g = tr.run(20000, 8)
+    o = oracle.run(arr, st, nphotons=20000, seed=8, policy=oracle.device_policy("fp64", st.grid_c()))
+    diff = {k: (g.stats[k], o.stats[k]) for k in COUNT_KEYS if g.stats[k] != o.stats[k]}
+    assert not diff, diff
+    assert g.stats["fresnel_events"] > 0
+    fluence_agrees(g.jmean, o.jmean)

@@ -202,3 +202,70 @@ def test_detector_kats(oracle):
     assert oracle.detector_bin(st, 2, (10, 0, 0), (-1, 0, 0), 1.0, 1) >= 0
     assert oracle.detector_bin(st, 2, (10, 0, 0), (1, 0, 0), 1.0, 1) < 0
     assert oracle.detector_bin(st, 0, (0, 0, 0), (1, 0, 0), 1.0, 2) < 0  # wrong layer
+
+
+# ---------------------------------------------------------------- SDF modifiers
+def _sph(r):
+    return S.sphere(r, S.mono(0.0, 0.0, 0.0, 1.0), 1)
+
+
+def test_bend_known_answers(oracle):
+    """test/SDF/test_SDF.f90:265-299 (test_bend): box(1,1,1) bent with k = 10."""
+    bbox = S.box((1.0, 1.0, 1.0), S.mono(0.0, 0.0, 0.0, 0.0), 1)
+    bent = S.FlatScene([S.bend(bbox, 10.0)])
+    plain = S.FlatScene([bbox])
+    d = oracle.eval_sdf(bent, [(0.0, 0.0, 0.0), (0.6, 0.0, 0.0), (0.4, -0.4, -0.4)])[:, 0]
+    assert d[0] < 0 and d[1] > 0 and d[2] > 0
+    assert oracle.eval_sdf(plain, [(0.4, -0.4, -0.4)])[0, 0] < 0
+
+
+def _points(n=200, seed=3, scale=2.0):
+    return np.random.default_rng(seed).uniform(-scale, scale, (n, 3))
+
+
+def test_revolution_of_sphere_is_torus(oracle):
+    pts = _points()
+    rev = oracle.eval_sdf(S.FlatScene([S.revolution(_sph(0.3), 1.1)]), pts)[:, 0]
+    tor = oracle.eval_sdf(S.FlatScene([S.torus(1.1, 0.3, S.mono(0, 0, 0, 1), 1)]), pts)[:, 0]
+    np.testing.assert_allclose(rev, tor, rtol=0, atol=1e-14)
+
+
+def test_onion_extrude_elongate_twist_formulas(oracle):
+    pts = _points()
+    r = np.linalg.norm(pts, axis=1)
+    got = oracle.eval_sdf(S.FlatScene([S.onion(_sph(0.8), 0.1)]), pts)[:, 0]
+    np.testing.assert_allclose(got, np.abs(r - 0.8) - 0.1, atol=1e-14)
+    got = oracle.eval_sdf(S.FlatScene([S.extrude(_sph(0.8), 0.3)]), pts)[:, 0]
+    d, wy = r - 0.8, np.abs(pts[:, 2]) - 0.3
+    want = np.minimum(np.maximum(d, wy), 0) + np.hypot(np.maximum(d, 0), np.maximum(wy, 0))
+    np.testing.assert_allclose(got, want, atol=1e-14)
+    # elongating a sphere along x gives a capsule (off the axis segment)
+    got = oracle.eval_sdf(S.FlatScene([S.elongate(_sph(0.3), (0.7, 0.0, 0.0))]), pts)[:, 0]
+    cap = oracle.eval_sdf(S.FlatScene([S.capsule((-0.7, 0, 0), (0.7, 0, 0), 0.3, S.mono(0, 0, 0, 1), 1)]), pts)[:, 0]
+    np.testing.assert_allclose(got, cap, atol=1e-14)
+    # zero twist / bend leave the primitive unchanged; a twist turns the point about z
+    box = S.box((1.0, 0.4, 2.0), S.mono(0, 0, 0, 1), 1)
+    base = oracle.eval_sdf(S.FlatScene([box]), pts)[:, 0]
+    for f in (S.twist, S.bend):
+        np.testing.assert_allclose(oracle.eval_sdf(S.FlatScene([f(box, 0.0)]), pts)[:, 0], base, atol=1e-15)
+    k = float(np.float32(0.7))
+    a = k * pts[:, 2]
+    rot = np.stack([np.cos(a) * pts[:, 0] - np.sin(a) * pts[:, 1], np.sin(a) * pts[:, 0] + np.cos(a) * pts[:, 1],
+                    pts[:, 2]], axis=1)
+    np.testing.assert_allclose(oracle.eval_sdf(S.FlatScene([S.twist(box, 0.7)]), pts)[:, 0],
+                               oracle.eval_sdf(S.FlatScene([box]), rot)[:, 0], atol=1e-14)
+
+
+def test_nested_modifiers_and_egg_preset(oracle):
+    """onion(revolution(egg)) is the reference's egg shell (setupGeometry.f90:37-38):
+    the outer modifier maps the point first, the inner one the value first."""
+    from signedmcrt_b200 import presets as P
+    arr = P.setup_egg()
+    pts = _points(100, 5, 4.0)
+    got = oracle.eval_sdf(S.FlatScene(arr), pts)
+    egg = S.egg(3.0, 3.0 * np.sqrt(2 - np.sqrt(2)), 3.0 * np.sqrt(2 - np.sqrt(2)), S.mono(0, 0, 0, 1), 1)
+    q = np.stack([np.hypot(pts[:, 0], pts[:, 2]) - 0.2, pts[:, 1], np.zeros(len(pts))], axis=1)
+    inner = oracle.eval_sdf(S.FlatScene([egg]), q)[:, 0]
+    np.testing.assert_allclose(got[:, 2], np.abs(inner) - 0.2, atol=1e-14)
+    with pytest.raises(ValueError):
+        S.onion(S.onion(S.onion(_sph(1.0), 0.1), 0.1), 0.1)
