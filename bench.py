@@ -285,6 +285,109 @@ def run_batch(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_render(args) -> None:
+    """render: the SDF voxel render (render_sub, src/sdfs/sdf_base.f90:302-346) of
+    the layered_vessels scene (8 regions: 3 boxes, 4 capsules, bounding box) on a
+    512^3 grid in FP64, the reference's arithmetic.  The 512 MiB FP32 image is
+    larger than L2.  Voxels/s; e2e through smcrt_render with the image copied to
+    pinned host memory; the reference arm is the oracle's OpenMP render loop."""
+    from signedmcrt_b200 import presets as P
+    from signedmcrt_b200.scene import FlatScene
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    n = int(round(args.packets ** (1.0 / 3.0))) if args.packets else 512
+    samples, extent = (n, n, n), (1.0, 1.0, 1.0)
+    flat = FlatScene(P.layered_vessels())
+    vox = n ** 3
+    metric, unit = "SDF voxel render throughput", "voxels/s"
+    workload = {"workload": f"render: layered_vessels scene (8 regions), {n}^3 voxels, FP64 SDF, FP32 image",
+                "render_size": list(samples), "extent": list(extent), "l2": "image 512 MiB > L2" if n >= 400 else
+                "image smaller than L2"}
+    from oracle import binding as O
+
+    def cpu_rate(target_s):
+        m = 64
+        t = time.perf_counter()
+        O.render(flat, (m, m, m), extent)
+        dt = time.perf_counter() - t
+        m = int(min(max(m * (target_s / max(dt, 1e-3)) ** (1 / 3), 64), n))
+        t = time.perf_counter()
+        O.render(flat, (m, m, m), extent)
+        dt = time.perf_counter() - t
+        return m ** 3 / dt, m, dt
+
+    if args.impl == "reference":
+        rate, m, dt = cpu_rate(args.ref_step_s)
+        times = []
+        for k in range(args.steps):
+            t = time.perf_counter()
+            O.render(flat, (m, m, m), extent)
+            times.append(time.perf_counter() - t)
+        v = m ** 3 * len(times) / sum(times)
+        print(json.dumps({"impl": "reference", "metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": dict(workload, sample=f"{m}^3 voxels per step"),
+                          "cpu_baseline": {"value": v, "unit": unit, "cores": O.max_threads(), "kind": "port",
+                                           "sample": f"{m}^3 voxels of the same grid extent per step"},
+                          "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+    from signedmcrt_b200 import transport as T
+    dev = torch.device("cuda", 0)
+    img = torch.empty(vox, dtype=torch.float32, device=dev)
+    s = torch.cuda.current_stream(dev)
+    for w in range(args.warmup):
+        T.render_device(flat, samples, extent, img.data_ptr(), stream=s.cuda_stream)
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for a, b in ev:
+            a.record(s)
+            T.render_device(flat, samples, extent, img.data_ptr(), stream=s.cuda_stream)
+            b.record(s)
+        torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
+    value = vox / (ms / 1e3)
+    # e2e: smcrt_render, device image allocated, rendered and copied to pinned host memory
+    host = torch.empty(vox, dtype=torch.float32, pin_memory=True).numpy()
+    e_times = []
+    for k in range(args.steps):
+        t = time.perf_counter()
+        T.check(T.lib().smcrt_render(flat.ptr(), T.PRECISIONS["fp64"],
+                                     np.asarray(samples, dtype=np.int32).ctypes.data_as(T.C.POINTER(T.C.c_int32)),
+                                     T.abi.dptr(np.asarray(extent, dtype=np.float64)),
+                                     host.ctypes.data_as(T.C.POINTER(T.C.c_float))))
+        e_times.append(time.perf_counter() - t)
+    e_ms = 1e3 * sum(e_times) / len(e_times)
+    regions, prims = flat.c.regions, flat.c.prims
+    flop_vox = sum(XFORM_FLOP + PRIM_FLOP[prims[regions[i].first_prim + j].kind]
+                   for i in range(flat.nregions) for j in range(regions[i].nprims)) + flat.nregions
+    pk = peaks()
+    fp64_peak = 148 * 64 * 2 * (pk["sm_max_mhz"] * 1e6) / 1e12
+    cpu_v, m, dt = (None, 0, 0.0) if args.no_cpu_baseline else cpu_rate(args.cpu_seconds)
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload,
+            "roofline": {"bound": "hbm", "achieved": 4 * vox / (ms / 1e3) / 1e9, "peak": pk["hbm_gbs"],
+                         "unit": "GB/s", "frac": 4 * vox / (ms / 1e3) / 1e9 / pk["hbm_gbs"], "traffic": None,
+                         "peak_source": pk["source"],
+                         "note": "the image write is the only DRAM stream; the kernel is bound by FP64 issue",
+                         "fp64_issue": {"flop_per_voxel": flop_vox,
+                                        "achieved_tflops": flop_vox * vox / (ms / 1e3) / 1e12,
+                                        "peak_tflops": fp64_peak,
+                                        "frac": flop_vox * vox / (ms / 1e3) / 1e12 / fp64_peak}},
+            "gpu_launches": args.steps, "clocks": clk.summary(),
+            "e2e": {"value": vox / (e_ms / 1e3), "unit": unit, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 4 * vox, "ms_per_step": e_ms,
+                    "path": "smcrt_render (C ABI): device image, render, copy to pinned host memory"},
+            "cpu_baseline": None if cpu_v is None else {
+                "value": cpu_v, "unit": unit, "cores": O.max_threads(), "kind": "port",
+                "sample": f"{m}^3 voxels, the oracle's OpenMP render loop, {dt:.1f} s"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args) -> None:
     """adjoint: layered_vessels, 1e7 packets; the path-replay gradient of a
     voxel-weighted fluence + detector loss w.r.t. 15 parameters (mu_a, mu_s, g of
@@ -380,7 +483,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="sphere_water",
-                    choices=["sphere_water", "box_slab", "layered_vessels", "batch256", "adjoint", "accuracy"])
+                    choices=["sphere_water", "box_slab", "layered_vessels", "batch256", "adjoint", "accuracy",
+                             "render"])
     ap.add_argument("--fd-batches", type=int, default=8, help="adjoint: batches of the finite-difference check")
     ap.add_argument("--fd-h", type=float, default=1e-3, help="adjoint: relative finite-difference step")
     ap.add_argument("--batch-scale", type=float, default=1.0, help="batch256: packet counts x this factor")
@@ -401,6 +505,9 @@ def main() -> None:
         return
     if args.config == "adjoint":
         run_adjoint(args)
+        return
+    if args.config == "render":
+        run_render(args)
         return
     if args.config == "accuracy":
         if int(os.environ.get("RANK", "0")) == 0 and args.impl != "reference":

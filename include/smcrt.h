@@ -374,6 +374,22 @@ int32_t smcrt_run_device_static(const smcrt_scene* scene, const smcrt_grid* grid
 /* Size of the static scratch array used by smcrt_run_device_static. */
 int64_t smcrt_static_scratch_bytes(void);
 
+/* ---- SDF voxel render (render_sub, src/sdfs/sdf_base.f90:302-346) ---------- */
+/* The minimum over all regions of the scene's signed distance at every voxel of a
+ * samples[0] x samples[1] x samples[2] grid: voxel (i, j, k), 1-based, sits at
+ * ((i - ns[0]) w[0], (j - ns[1]) w[1], (k - ns[2]) w[2]) with ns = nint(samples / 2)
+ * and w = extent / ns.  Written FP32 in Fortran order (i fastest) to `image`, host
+ * memory of samples[0]*samples[1]*samples[2] floats.  Replaces the OpenMP loop of
+ * render_sub; the caller writes the file (write_data).  precision: SMCRT_FP64
+ * evaluates in double as the reference's real(wp) does, SMCRT_FP32 in float.
+ * Each samples[a] in [1, 65536]. */
+int32_t smcrt_render(const smcrt_scene* scene, int32_t precision, const int32_t samples[3],
+                     const double extent[3], float* image);
+/* The same into caller DEVICE memory, asynchronously on `stream` (a cudaStream_t;
+ * NULL = the default stream).  Allocates nothing. */
+int32_t smcrt_render_device(const smcrt_scene* scene, int32_t precision, const int32_t samples[3],
+                            const double extent[3], float* image_dev, void* stream);
+
 /* ---- device-function probes (parity of the building blocks) --------------- */
 /* Evaluates every region's SDF at npts points (xyz triples); out[p*nregions+r]. */
 int32_t smcrt_eval_sdf(const smcrt_scene* scene, int32_t precision,

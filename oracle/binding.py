@@ -67,6 +67,7 @@ def lib() -> C.CDLL:
             "oracle_eval_sdf": ([P(abi.Scene), C.c_int32, P(C.c_double), C.c_int64, P(C.c_double)], C.c_int32),
             "oracle_calc_normal": ([P(abi.Scene), C.c_int32, C.c_double, P(C.c_double), C.c_int64,
                                     P(C.c_double)], C.c_int32),
+            "oracle_render": ([P(abi.Scene), C.c_int32, P(C.c_int32), P(C.c_double), P(C.c_float)], C.c_int32),
             "oracle_fresnel": ([C.c_int32, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double),
                                 C.c_int64, P(C.c_double)], C.c_int32),
             "oracle_reflect_refract": ([C.c_int32, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double),
@@ -134,6 +135,17 @@ def eval_sdf(flat: FlatScene, pts, precision: str = "fp64") -> np.ndarray:
     assert lib().oracle_eval_sdf(flat.ptr(), abi.FP32 if precision == "fp32" else abi.FP64, abi.dptr(pts),
                                  len(pts), abi.dptr(out)) == 0
     return out
+
+
+def render(flat: FlatScene, samples, extent, precision: str = "fp64") -> np.ndarray:
+    """render_sub (src/sdfs/sdf_base.f90:302-346): the FP32 voxel image, shape samples."""
+    ns = np.ascontiguousarray(samples, dtype=np.int32)
+    ext = np.ascontiguousarray(extent, dtype=np.float64)
+    img = np.empty(int(np.prod(ns, dtype=np.int64)), dtype=np.float32)
+    assert lib().oracle_render(flat.ptr(), abi.FP32 if precision == "fp32" else abi.FP64,
+                               ns.ctypes.data_as(C.POINTER(C.c_int32)), abi.dptr(ext),
+                               img.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    return img.reshape(tuple(int(x) for x in ns), order="F")
 
 
 def calc_normal(flat: FlatScene, region0: int, pts, h: float = 1e-6) -> np.ndarray:

@@ -1211,6 +1211,37 @@ V3<R> v3(const double* p) { return V3<R>{(R)p[0], (R)p[1], (R)p[2]}; }
 }  // namespace
 
 // ===========================================================================
+// render_sub, src/sdfs/sdf_base.f90:302-346: ns = nint(samples / 2) (:320),
+// wid = extent / ns (:322), voxel (i, j, k) at ((i - ns) wid) (:326-331), the
+// minval over regions (:332-336) stored as real(sp), image(i, j, k) column-major.
+template <class R>
+static void render_t(const smcrt_scene* scene, const int32_t* samples, const double* extent, float* image) {
+    const Scene<R> sc = make_scene<R>(scene);
+    double ns[3], wid[3];
+    for (int a = 0; a < 3; ++a) {
+        ns[a] = std::round(samples[a] / 2.0);  // nint: half away from zero
+        wid[a] = extent[a] / ns[a];
+    }
+    const int64_t n0 = samples[0], n1 = samples[1], n2 = samples[2];
+#pragma omp parallel for schedule(dynamic)
+    for (int64_t k = 1; k <= n2; ++k) {
+        const double z = ((double)k - ns[2]) * wid[2];
+        for (int64_t j = 1; j <= n1; ++j) {
+            const double y = ((double)j - ns[1]) * wid[1];
+            for (int64_t i = 1; i <= n0; ++i) {
+                const double x = ((double)i - ns[0]) * wid[0];
+                const V3<R> pos{(R)x, (R)y, (R)z};
+                R d = eval_region(sc, 0, pos);
+                for (int r = 1; r < scene->nregions; ++r) {
+                    const R e = eval_region(sc, r, pos);
+                    if (e < d) d = e;
+                }
+                image[(i - 1) + n0 * ((j - 1) + n1 * (k - 1))] = (float)d;
+            }
+        }
+    }
+}
+
 extern "C" {
 
 int32_t oracle_max_threads(void) {
@@ -1300,6 +1331,16 @@ int32_t oracle_eval_sdf(const smcrt_scene* scene, int32_t precision, const doubl
         for (int64_t p = 0; p < npts; ++p)
             for (int r = 0; r < nr; ++r) out[p * nr + r] = eval_region(sc, r, v3<double>(pts + 3 * p));
     }
+    return SMCRT_OK;
+}
+
+int32_t oracle_render(const smcrt_scene* scene, int32_t precision, const int32_t* samples, const double* extent,
+                      float* image) {
+    if (validate_scene(scene) || !samples || !extent || !image) return SMCRT_ERR_ARG;
+    for (int a = 0; a < 3; ++a)
+        if (samples[a] < 1) return SMCRT_ERR_ARG;
+    if (precision == SMCRT_FP32) render_t<float>(scene, samples, extent, image);
+    else render_t<double>(scene, samples, extent, image);
     return SMCRT_OK;
 }
 

@@ -42,6 +42,10 @@ int64_t oracle_detector_bins(const smcrt_detector* dets, int32_t ndet);
 
 int32_t oracle_eval_sdf(const smcrt_scene* scene, int32_t precision, const double* pts,
                         int64_t npts, double* out);
+/* render_sub (src/sdfs/sdf_base.f90:302-346): min over regions at every voxel,
+ * FP32, Fortran order; samples[3] voxels, extent[3] half-widths. */
+int32_t oracle_render(const smcrt_scene* scene, int32_t precision, const int32_t* samples,
+                      const double* extent, float* image);
 int32_t oracle_calc_normal(const smcrt_scene* scene, int32_t region0, double h,
                            const double* pts, int64_t npts, double* out_xyz);
 int32_t oracle_fresnel(int32_t precision, const double* I, const double* N, const double* n1,

@@ -169,6 +169,10 @@ SIGNATURES = {
                        C.c_int32),
     "smcrt_calc_normal": ([C.POINTER(Scene), C.c_int32, C.c_double, C.POINTER(C.c_double), C.c_int64,
                            C.POINTER(C.c_double)], C.c_int32),
+    "smcrt_render": ([C.POINTER(Scene), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                      C.POINTER(C.c_float)], C.c_int32),
+    "smcrt_render_device": ([C.POINTER(Scene), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                             C.c_void_p, C.c_void_p], C.c_int32),
     "smcrt_fresnel": ([C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                        C.POINTER(C.c_double), C.c_int64, C.POINTER(C.c_double)], C.c_int32),
     "smcrt_reflect_refract": ([C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),

@@ -57,6 +57,9 @@ def _units() -> list[tuple[Path, list[str]]]:
     for name in ("smcrt_probes", "smcrt_api"):
         obj = BUILD / f"{name}.o"
         units.append((obj, ["-c", str(CSRC / f"{name}.cu"), "-o", str(obj)]))
+    # the render follows the CPU restatement operation for operation in FP64
+    obj = BUILD / "smcrt_render.o"
+    units.append((obj, ["--fmad=false", "-c", str(CSRC / "smcrt_render.cu"), "-o", str(obj)]))
     return units
 
 

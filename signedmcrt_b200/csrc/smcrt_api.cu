@@ -1470,6 +1470,50 @@ int32_t smcrt_calc_normal(const smcrt_scene* scene, int32_t region0, double h, c
     return SMCRT_OK;
 }
 
+static int render_args(const smcrt_scene* scene, int32_t precision, const int32_t* samples, const double* extent,
+                       const void* image, long long& total) {
+    int rc = validate_scene(scene);
+    if (rc) return rc;
+    if (!samples || !extent || !image) return fail(SMCRT_ERR_ARG, "render: null pointer");
+    if (precision != SMCRT_FP32 && precision != SMCRT_FP64) return fail(SMCRT_ERR_ARG, "render: bad precision");
+    total = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (samples[a] < 1 || samples[a] > 65536) return fail(SMCRT_ERR_ARG, "render: samples out of [1, 65536]");
+        if (!std::isfinite(extent[a])) return fail(SMCRT_ERR_ARG, "render: extent not finite");
+        total *= samples[a];
+    }
+    return SMCRT_OK;
+}
+
+int32_t smcrt_render(const smcrt_scene* scene, int32_t precision, const int32_t samples[3], const double extent[3],
+                     float* image) {
+    g_err.clear();
+    long long total = 0;
+    int rc = render_args(scene, precision, samples, extent, image, total);
+    if (rc) return rc;
+    int dev, nsm;
+    rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    DBuf dimg;
+    UP(dimg, nullptr, sizeof(float) * total);
+    CK(launch_render(precision, scene, samples, extent, (float*)dimg.p, nsm, 0));
+    CK(cudaMemcpy(image, dimg.p, sizeof(float) * total, cudaMemcpyDeviceToHost));
+    return SMCRT_OK;
+}
+
+int32_t smcrt_render_device(const smcrt_scene* scene, int32_t precision, const int32_t samples[3],
+                            const double extent[3], float* image_dev, void* stream) {
+    g_err.clear();
+    long long total = 0;
+    int rc = render_args(scene, precision, samples, extent, image_dev, total);
+    if (rc) return rc;
+    int dev, nsm;
+    rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    CK(launch_render(precision, scene, samples, extent, image_dev, nsm, (cudaStream_t)stream));
+    return SMCRT_OK;
+}
+
 static int fresnel_common(int32_t precision, const double* I, const double* N, const double* n1, const double* n2,
                           const double* u, int64_t n, double* R, double* Iout, int32_t* refl) {
     if (!I || !N || !n1 || !n2 || n < 0) return fail(SMCRT_ERR_ARG, "fresnel: bad arguments");

@@ -35,6 +35,11 @@ cudaError_t probe_scatter(int precision, const double* dir, const double* g, con
                           double* out);
 cudaError_t probe_philox(const uint32_t* key, const uint32_t* ctr, long long n, uint32_t* out);
 
+// SDF voxel render into a device image of samples[0]*samples[1]*samples[2]
+// floats, Fortran order (smcrt_render.cu).
+cudaError_t launch_render(int precision, const smcrt_scene* scene, const int samples[3], const double extent[3],
+                          float* d_img, int nsm, cudaStream_t s);
+
 // Scene conversion shared by the API and the probes.
 template <class R>
 void fill_scene(SceneT<R>& d, const smcrt_scene* s);

@@ -24,7 +24,7 @@ import numpy as np
 from . import writer
 from .config import Settings, parse_params
 from .presets import setup_simulation
-from .transport import Transport
+from .transport import Transport, render
 
 
 @dataclass
@@ -60,6 +60,12 @@ def run_kernel(settings: Settings, kernel: str, *, end_early: bool = False, inpu
     sim = st.simulation
     base = writer.data_dirs(root) if write else None
     files = []
+    if st.output.render_geom:  # setup, src/kernelsMod.f90:531-536
+        if verbose:
+            print("Rendering geometry to file")
+        image = render_geometry(arr, st)
+        if write:
+            files.append(writer.write_data(image, base / st.output.render, overwrite=True))
     with Transport(arr, st, kernel=kernel, precision=precision, end_early=end_early) as tr:
         every = int(sim.checkpoint_every_n)
         chunked = write and 0 < every < nphotons
@@ -103,6 +109,13 @@ def run_kernel(settings: Settings, kernel: str, *, end_early: bool = False, inpu
         if st.detectors:
             files += writer.write_detected_photons(st, bins, base / "detectors")
     return KernelRun(jmean, fluence, bins, nscatt, stats, files)
+
+
+def render_geometry(array, settings: Settings) -> np.ndarray:
+    """render_vec (src/sdfs/sdf_base.f90:287-299): the scene rendered on a
+    render_size voxel grid spanning the fluence grid's half-widths."""
+    g = settings.grid
+    return render(array, settings.output.render_size, (g.xmax, g.ymax, g.zmax))
 
 
 def pathlength_scatter(input_file: str | Path, **kw) -> KernelRun:

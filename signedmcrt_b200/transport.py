@@ -261,6 +261,37 @@ def run_batched(transports: list, nphotons, seeds):
             for i, (t, j, b) in enumerate(zip(transports, jms, bins))]
 
 
+# ---------------------------------------------------------------------- render
+def _render_args(samples, extent):
+    ns = np.ascontiguousarray([int(x) for x in samples], dtype=np.int32)
+    ext = np.ascontiguousarray([float(x) for x in extent], dtype=np.float64)
+    if ns.shape != (3,) or ext.shape != (3,):
+        raise ValueError("render: samples and extent need 3 entries")
+    return ns, ext
+
+
+def render(array, samples, extent, precision: str = "fp64") -> np.ndarray:
+    """render_sub (src/sdfs/sdf_base.f90:302-346) on the device: the minimum over
+    regions of the signed distance on a samples[0] x samples[1] x samples[2] voxel
+    grid spanning [-extent, extent] (voxel i at (i - nint(n/2)) * extent / nint(n/2)),
+    FP32, shape `samples`, Fortran order."""
+    flat = array if isinstance(array, FlatScene) else FlatScene(array)
+    ns, ext = _render_args(samples, extent)
+    img = np.empty(int(np.prod(ns, dtype=np.int64)), dtype=np.float32)
+    check(lib().smcrt_render(flat.ptr(), PRECISIONS[precision], ns.ctypes.data_as(C.POINTER(C.c_int32)),
+                             abi.dptr(ext), img.ctypes.data_as(C.POINTER(C.c_float))))
+    return img.reshape(tuple(int(x) for x in ns), order="F")
+
+
+def render_device(array, samples, extent, image_ptr: int, precision: str = "fp64", stream: int = 0) -> None:
+    """The render into caller device memory (a float buffer of prod(samples)
+    entries, Fortran order), asynchronously on `stream`."""
+    flat = array if isinstance(array, FlatScene) else FlatScene(array)
+    ns, ext = _render_args(samples, extent)
+    check(lib().smcrt_render_device(flat.ptr(), PRECISIONS[precision], ns.ctypes.data_as(C.POINTER(C.c_int32)),
+                                    abi.dptr(ext), C.c_void_p(image_ptr), C.c_void_p(stream or None)))
+
+
 # ---------------------------------------------------------------------- probes
 def eval_sdf(flat: FlatScene, pts: np.ndarray, precision: str = "fp32") -> np.ndarray:
     pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)

@@ -93,3 +93,23 @@ def test_struct_layout_matches_header(tmp_path):
         assert C.sizeof(cls) == layout[name]["size"], name
         for f in fields:
             assert getattr(cls, f).offset == layout[name][f], (name, f)
+
+
+def test_render_checks_its_arguments_before_the_device():
+    """smcrt_render rejects bad sizes and extents with SMCRT_ERR_ARG whether or not a
+    GPU is visible; without one a valid call reports SMCRT_ERR_NO_DEVICE."""
+    import torch
+    from signedmcrt_b200 import _lib, presets as P, transport as T
+    arr = P.setup_egg()
+    for samples, extent in (((0, 4, 4), (1.0, 1.0, 1.0)), ((4, 70000, 4), (1.0, 1.0, 1.0)),
+                            ((4, 4, 4), (1.0, float("nan"), 1.0))):
+        with pytest.raises(_lib.SmcrtError) as e:
+            T.render(arr, samples, extent)
+        assert e.value.code == abi.ERR_ARG
+    with pytest.raises(_lib.SmcrtError) as e:
+        T.render_device(arr, (4, 4, 4), (1.0, 1.0, 1.0), 0)
+    assert e.value.code == abi.ERR_ARG  # null image pointer
+    if not torch.cuda.is_available():
+        with pytest.raises(_lib.SmcrtError) as e:
+            T.render(arr, (4, 4, 4), (1.0, 1.0, 1.0))
+        assert e.value.code == abi.ERR_NO_DEVICE

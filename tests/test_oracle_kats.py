@@ -269,3 +269,40 @@ def test_nested_modifiers_and_egg_preset(oracle):
     np.testing.assert_allclose(got[:, 2], np.abs(inner) - 0.2, atol=1e-14)
     with pytest.raises(ValueError):
         S.onion(S.onion(S.onion(_sph(1.0), 0.1), 0.1), 0.1)
+
+
+def _render_restated(oracle, flat, samples, extent, precision="fp64"):
+    """render_sub (src/sdfs/sdf_base.f90:319-336) with numpy building the voxel
+    centres and the oracle evaluating them, image(i, j, k) in Fortran order."""
+    ns = np.floor(np.asarray(samples) / 2.0 + 0.5)  # nint, half away from zero
+    w = np.asarray(extent, dtype=np.float64) / ns
+    axes = [(np.arange(1, n + 1, dtype=np.float64) - ns[a]) * w[a] for a, n in enumerate(samples)]
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    pts = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
+    d = oracle.eval_sdf(flat, pts, precision).min(axis=1).astype(np.float32)
+    return d.reshape(tuple(samples), order="F")
+
+
+def test_render_voxel_centres_known_answers(oracle):
+    """A unit sphere on a 3^3 render of half-width 1: nint(3/2) = 2 puts the voxels
+    at -0.5, 0, 0.5 (sdf_base.f90:320-331)."""
+    img = oracle.render(S.FlatScene([_sph(1.0)]), (3, 3, 3), (1.0, 1.0, 1.0))
+    assert img.dtype == np.float32 and img.shape == (3, 3, 3)
+    assert img[1, 1, 1] == np.float32(-1.0)
+    assert img[2, 1, 1] == np.float32(-0.5)
+    assert img[0, 0, 0] == np.float32(np.sqrt(0.75) - 1.0)
+    # even sizes: nint(4/2) = 2, voxels at -0.5, 0, 0.5, 1.0
+    img = oracle.render(S.FlatScene([_sph(1.0)]), (4, 1, 1), (1.0, 1.0, 1.0))
+    np.testing.assert_array_equal(img[:, 0, 0], np.float32([-0.5, -1.0, -0.5, 0.0]))
+
+
+@pytest.mark.parametrize("scene", ["sphere_water", "layered_vessels", "test_egg"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_render_matches_restatement(oracle, scene, precision):
+    """The oracle's render loop against the restatement above, ragged sizes, bit for bit."""
+    arr = P.setup_egg() if scene == "test_egg" else P.setup_simulation(P.benchmark_settings(scene))
+    flat = S.FlatScene(arr)
+    for samples in ((9, 6, 5), (7, 1, 4)):
+        want = _render_restated(oracle, flat, samples, (2.0, 1.5, 1.0), precision)
+        got = oracle.render(flat, samples, (2.0, 1.5, 1.0), precision)
+        np.testing.assert_array_equal(got, want)
