@@ -1092,6 +1092,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     __shared__ int s_off[kGroups][Q][NW];
     __shared__ unsigned short s_list[SlotCount<R>::n];
     __shared__ int s_stop;
+    __shared__ int s_next;  // next unclaimed 32-item chunk of the round's list
     extern __shared__ __align__(16) unsigned char s_dyn[];
     Slots<R>& sl = *reinterpret_cast<Slots<R>*>(s_dyn);
     unsigned* s_bins = reinterpret_cast<unsigned*>(s_dyn + slots_bytes<R>());
@@ -1140,6 +1141,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
                 stop = 1;
             }
             s_stop = stop;
+            s_next = NW;
         }
         __syncthreads();
         // every warp scans the (group, q, warp) counts itself: each group is
@@ -1183,11 +1185,22 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         __syncthreads();
         if (total == 0 || stop) break;
         // ---- one pass per listed packet: warp w takes 32-item chunks w, w + NW, ...
-        for (int i = t; i < total; i += kBlock) {
-            const int s = s_list[i];
-            int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc);
-            store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
+        // warp w takes chunk w, so the chunks at the head of the list (the FP64
+        // near-surface group) land on different warps; later chunks go to the
+        // warps that finish first
+        const int nchunks = (total + 31) >> 5;
+        for (int chunk = warp; chunk < nchunks;) {
+            const int i = chunk * 32 + (int)lane;
+            if (i < total) {
+                const int s = s_list[i];
+                int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
+                transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins,
+                                                                    s_acc);
+                store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
+            }
+            int next = 0;
+            if (lane == 0) next = atomicAdd(&s_next, 1);
+            chunk = __shfl_sync(0xffffffffu, next, 0);
         }
     }
     // events of packets still in flight (time budget) and since the last retire
