@@ -906,14 +906,16 @@ struct SlotCount {
 };
 // Sort groups of the actions a packet can wait in between rounds, in list
 // order: FP64 near-surface sweep, sweep (or a pending crossing), walk, interact,
-// retire/launch.  With the chunk assignment below the costly FP64 chunks are some
-// warps' first chunk, and a warp's two chunks come from different parts of the
-// list, so the warps of a CTA run a mix of actions at any time.  (Of the orders
-// measured this one was fastest on all three benchmark scenes; ordering by pass
-// cost, or pairing cheap with expensive chunks, was slower.)  A_DONE maps to
-// kGroups (not listed).
+// retire/launch.  Each warp's first chunk is fixed (warp w, chunk w), so the
+// costly FP64 chunks at the head of the list go to different warps; the rest of
+// the list goes to whichever warp finishes first.  A_DONE maps to kGroups (not
+// listed).
+// Nibble `act` of SMCRT_GROUP_ORDER is the group of action `act`.
+#ifndef SMCRT_GROUP_ORDER
+#define SMCRT_GROUP_ORDER 0x05431214u
+#endif
 constexpr int kGroups = 5;
-__device__ __forceinline__ int act_group(int act) { return (int)((0x05431214u >> (4 * act)) & 0xFu); }
+__device__ __forceinline__ int act_group(int act) { return (int)((SMCRT_GROUP_ORDER >> (4 * act)) & 0xFu); }
 
 template <class R, int kSlots = SlotCount<R>::n>
 struct Slots {
