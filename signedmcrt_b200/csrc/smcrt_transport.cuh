@@ -273,7 +273,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define SMCRT_MIN_BLOCKS 1
 #endif
 #ifndef SMCRT_WALK_SEGMENTS
-#define SMCRT_WALK_SEGMENTS 4
+#define SMCRT_WALK_SEGMENTS 3
 #endif
 
 // Per-lane actions of the flattened transport loop.
