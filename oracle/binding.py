@@ -64,6 +64,9 @@ def lib() -> C.CDLL:
                             C.c_int32, P(Policy), C.c_int64, C.c_int64, C.c_uint64, C.c_uint32, P(C.c_double),
                             P(C.c_int64), P(C.c_double), P(C.c_double), P(abi.Stats), C.c_void_p], C.c_int32),
             "oracle_detector_bins": ([P(abi.Detector), C.c_int32], C.c_int64),
+            "oracle_adjoint": ([P(abi.Scene), P(abi.Grid), P(abi.Source), P(abi.Detector), C.c_int32, P(Policy),
+                                C.c_int64, C.c_uint64, P(C.c_double), P(C.c_double), P(C.c_int32), C.c_int32,
+                                P(C.c_double)], C.c_int32),
             "oracle_eval_sdf": ([P(abi.Scene), C.c_int32, P(C.c_double), C.c_int64, P(C.c_double)], C.c_int32),
             "oracle_calc_normal": ([P(abi.Scene), C.c_int32, C.c_double, P(C.c_double), C.c_int64,
                                     P(C.c_double)], C.c_int32),
@@ -127,6 +130,31 @@ def run(array, st: Settings, *, nphotons: int, seed: int, policy: Policy | None 
         raise RuntimeError(f"oracle_run failed ({rc})")
     return OracleResult(jm.reshape((g.nxg, g.nyg, g.nzg), order="F") if jm is not None else None, bins[:nb],
                         stats.to_dict(), states[:nphotons] if states is not None else None)
+
+
+def adjoint(array, st: Settings, *, nphotons: int, seed: int, w, h, region_group, ngroups: int,
+            policy: Policy | None = None) -> tuple[np.ndarray, float]:
+    """Perturbation Monte Carlo reference gradient of L = sum_v w[v] jmean[v] +
+    sum_b h[b] bins[b] over packets [0, nphotons) of the pathlength kernel:
+    (grad (3, ngroups) -- rows d/d mua, d/d mus, d/d g of each group, summed over
+    packets -- and L).  w: voxel weights in Fortran order (nxg, nyg, nzg); h: bin
+    weights or None."""
+    flat = array if isinstance(array, FlatScene) else FlatScene(array)
+    grid, src = st.grid_c(), st.source_c()
+    dets = st.detectors_c()
+    darr = (abi.Detector * max(1, len(dets)))(*dets)
+    pol = policy if policy is not None else reference_policy()
+    wv = np.ascontiguousarray(np.asarray(w, dtype=np.float64).reshape(-1, order="F"))
+    if wv.size != st.grid.nxg * st.grid.nyg * st.grid.nzg:
+        raise ValueError("adjoint: w needs one weight per voxel")
+    hv = None if h is None else np.ascontiguousarray(h, dtype=np.float64)
+    rg = np.ascontiguousarray(region_group, dtype=np.int32)
+    out = np.zeros(3 * ngroups + 1)
+    rc = lib().oracle_adjoint(flat.ptr(), C.byref(grid), C.byref(src), darr, len(dets), C.byref(pol), nphotons,
+                              seed, abi.dptr(wv), abi.dptr(hv), abi.i32ptr(rg), ngroups, abi.dptr(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_adjoint failed ({rc})")
+    return out[: 3 * ngroups].reshape(3, ngroups), float(out[3 * ngroups])
 
 
 def eval_sdf(flat: FlatScene, pts, precision: str = "fp64") -> np.ndarray:

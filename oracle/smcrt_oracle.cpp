@@ -423,7 +423,10 @@ struct GridD {
 struct Tally {
     double* j64 = nullptr;
     float* j32 = nullptr;
+    const double* w = nullptr;  // perturbation MC: voxel weights of the loss
+    double* csum = nullptr;     // and the packet's weighted path length
     void add(int64_t idx, double v) {
+        if (csum) *csum += w[idx] * v;
         if (j32) {
             float* a = j32 + idx;
 #pragma omp atomic
@@ -436,10 +439,13 @@ struct Tally {
     }
 };
 
+constexpr int kAdjGroups = 16;
 struct Counters {
     uint64_t sdf = 0, vox = 0, steps = 0, scat = 0, fres = 0, refl = 0, stepcap = 0, err = 0, draws = 0;
     double nscatt = 0;
     double mom[24] = {0};
+    double adj[3 * kAdjGroups] = {0};  // perturbation MC: sum over packets of C * score
+    double loss = 0;                   // and of C
 };
 
 template <class R>
@@ -625,9 +631,12 @@ bool boundary_event(const Scene<E>& scE, int which, int L, int nl, V3<double> po
 }
 
 // tauint2, src/inttau2.f90:15-210
+// len (perturbation MC, optional): path length per region of the flights traced,
+// added to; by_tau: whether the last flight ended at its optical depth (an
+// interaction), not at an escape or a kill.
 template <class R, class Rng>
 void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, const Pol& pol, Packet<R>& pk, Rng& rng,
-             Tally& t, Counters& c) {
+             Tally& t, Counters& c, double* len = nullptr, bool* by_tau = nullptr) {
     const int N = (int)sc.regions.size();
     V3<double> pos = pk.pos, oldpos = pos;
     V3<R> dir = pk.dir;
@@ -657,6 +666,7 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
             R tsdf = dsdf * kap;
             if (taurun + tsdf <= tau) {
                 taurun = taurun + tsdf;
+                if (len) len[pk.layer] += (double)dsdf;
                 oldpos = pos;
                 ok = pol.ref_dda ? update_grids_ref(g, cv<R>(oldpos), dir, dsdf, (R)pol.delta, t, c, pk.tflag)
                                  : update_grids_int(g, cv<R>(oldpos), dir, dsdf, t, c, pk.tflag);
@@ -664,6 +674,7 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
             } else {
                 dsdf = (tau - taurun) / kap;
                 taurun = tau;
+                if (len) len[pk.layer] += (double)dsdf;
                 oldpos = pos;
                 pos = advance(pos, dsdf, dir);
                 ok = pol.ref_dda ? update_grids_ref(g, cv<R>(oldpos), dir, dsdf, (R)pol.delta, t, c, pk.tflag)
@@ -766,6 +777,7 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
         }
         if (pk.tflag) break;
     }
+    if (by_tau) *by_tau = taurun >= tau;
     pk.pos = pos;
     pk.dir = dir;
     if (std::fabs(pos.x) > g.xmax) pk.tflag = true;
@@ -812,7 +824,7 @@ inline void phi_angles(double u, double& cosp, double& sinp) {
 }
 
 template <class R, class Rng>
-void scatter(V3<R>& dir, R hgg, R g2, Rng& rng) {
+void scatter(V3<R>& dir, R hgg, R g2, Rng& rng, double* cost_out = nullptr) {
     const R one = 1;
     R cost, sint;
     if (hgg == (R)0) {
@@ -821,6 +833,7 @@ void scatter(V3<R>& dir, R hgg, R g2, Rng& rng) {
         (void)rng.next();  // ran2() < p with p = 0 (:739)
         hg_angles(hgg, g2, rng.next(), cost, sint);
     }
+    if (cost_out) *cost_out = (double)cost;
     R cosp, sinp;
     phi_angles(rng.next(), cosp, sinp);
     R uxx, uyy, uzz;
@@ -1067,16 +1080,70 @@ struct RunArgs {
     Tally tally;
     double* bins;
     smcrt_packet_state* states;
+    const struct AdjArgs* adj = nullptr;  // perturbation MC gradient (pathlength kernel)
 };
+
+// Perturbation Monte Carlo (likelihood-ratio) reference gradient of
+// L = sum_v w[v] jmean[v] + sum_b h[b] bins[b] with respect to each region
+// group's (mua, mus, g): per packet, its contribution C to L times the derivative
+// of the log density of its whole path.  That density is, per flight, the
+// survival exp(-kappa l) in every region crossed and, where the flight ends at
+// its optical depth, the interaction density kappa; per interaction the roulette
+// probability mus/kappa (scatter) or mua/kappa (absorption); per scatter the
+// Henyey-Greenstein density of the sampled cos(theta).  Fresnel choices and
+// emission do not depend on these parameters.
+struct AdjArgs {
+    const double* w;        // voxel weights, nxg*nyg*nzg
+    const double* h;        // detector bin weights or null
+    const int32_t* group;   // region -> group, -1: not differentiated
+    int ngroups;
+};
+
+// d/dg log p_HG(mu; g), p_HG = (1 - g^2) / (2 (1 + g^2 - 2 g mu)^(3/2))
+inline double hg_score(double g, double mu) {
+    return -2.0 * g / (1.0 - g * g) - 3.0 * (g - mu) / (1.0 + g * g - 2.0 * g * mu);
+}
 
 template <class R, class Rng>
 void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, const RunArgs& A, Rng& rng,
                 Counters& c, int64_t pid) {
     Tally t = A.tally;
     Packet<R> pk{};
+    const AdjArgs* adj = (A.kernel == SMCRT_KERNEL_PATHLENGTH) ? A.adj : nullptr;
+    double C = 0, S[3][kAdjGroups] = {};
+    thread_local std::vector<double> len;
+    double* lp = nullptr;
+    bool by_tau = false;
+    if (adj) {
+        t.w = adj->w;
+        t.csum = &C;
+        len.assign(sc.regions.size(), 0.0);
+        lp = len.data();
+    }
+    auto mua_of = [&](int r) { return A.scene->regions[r].mua; };
+    auto mus_of = [&](int r) { return A.scene->regions[r].mus; };
+    // score of the flights just traced: survival per region, and the interaction
+    // density where the last flight ended at its optical depth
+    auto flights = [&]() {
+        for (size_t r = 0; r < len.size(); ++r) {
+            const int gi = adj->group[r];
+            if (gi >= 0 && len[r] != 0.0) {
+                S[0][gi] -= len[r];
+                S[1][gi] -= len[r];
+            }
+            len[r] = 0.0;
+        }
+        const int gi = adj->group[pk.layer];
+        if (by_tau && gi >= 0) {
+            const double k = mua_of(pk.layer) + mus_of(pk.layer);
+            S[0][gi] += 1.0 / k;
+            S[1][gi] += 1.0 / k;
+        }
+    };
     emit(*A.src, g, pk, rng);
     pk.layer = launch_layer(sc, cv<R>(pk.pos), c);
-    tauint2(sc, sc64, g, A.pol, pk, rng, t, c);
+    tauint2(sc, sc64, g, A.pol, pk, rng, t, c, lp, adj ? &by_tau : nullptr);
+    if (adj) flights();
     if (A.kernel == SMCRT_KERNEL_WEIGHT) {  // weight_scatter :99-134
         while (!pk.tflag) {
             const Region<R>& rg = sc.regions[pk.layer];
@@ -1104,8 +1171,17 @@ void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, c
         while (!pk.tflag) {
             R ran = rng.next();
             const Region<R>& rg = sc.regions[pk.layer];
+            const int gi = adj ? adj->group[pk.layer] : -1;
             if (ran < rg.albedo) {
-                scatter(pk.dir, rg.hgg, rg.g2, rng);
+                double mu = 0.0;
+                scatter(pk.dir, rg.hgg, rg.g2, rng, adj ? &mu : nullptr);
+                if (gi >= 0) {  // roulette mus/kappa, then the phase function
+                    const double k = mua_of(pk.layer) + mus_of(pk.layer);
+                    S[0][gi] -= 1.0 / k;
+                    S[1][gi] += 1.0 / mus_of(pk.layer) - 1.0 / k;
+                    const double hg = A.scene->regions[pk.layer].hgg;
+                    S[2][gi] += (hg == 0.0) ? 3.0 * mu : hg_score(hg, mu);
+                }
                 ++c.scat;
                 c.nscatt += 1.0;
                 pk.nscatt += 1;
@@ -1124,10 +1200,16 @@ void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, c
                     }
                 }
             } else {
+                if (gi >= 0) {  // roulette mua/kappa
+                    const double k = mua_of(pk.layer) + mus_of(pk.layer);
+                    S[0][gi] += 1.0 / mua_of(pk.layer) - 1.0 / k;
+                    S[1][gi] -= 1.0 / k;
+                }
                 pk.tflag = true;
                 break;
             }
-            tauint2(sc, sc64, g, A.pol, pk, rng, t, c);
+            tauint2(sc, sc64, g, A.pol, pk, rng, t, c, lp, adj ? &by_tau : nullptr);
+            if (adj) flights();
         }
     }
     // detectors (:302-306 / :136-140)
@@ -1143,8 +1225,14 @@ void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, c
                 double* a = A.bins + b;
 #pragma omp atomic
                 *a += 1.0;
+                if (adj && adj->h) C += adj->h[b];
             }
         }
+    }
+    if (adj) {
+        for (int k = 0; k < 3; ++k)
+            for (int gi = 0; gi < adj->ngroups; ++gi) c.adj[k * kAdjGroups + gi] += C * S[k][gi];
+        c.loss += C;
     }
     c.draws += (uint64_t)rng.ndraws;
     if (A.states) {
@@ -1160,7 +1248,7 @@ void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, c
 }
 
 template <class R>
-void run_all(const RunArgs& A, smcrt_stats* st, int threads) {
+void run_all(const RunArgs& A, smcrt_stats* st, int threads, double* adj_out = nullptr) {
     Scene<R> sc = make_scene<R>(A.scene);
     Scene<double> sc64 = make_scene<double>(A.scene);
     GridD g(*A.grid);
@@ -1186,7 +1274,15 @@ void run_all(const RunArgs& A, smcrt_stats* st, int threads) {
             tot.fres += c.fres; tot.refl += c.refl; tot.stepcap += c.stepcap; tot.err += c.err;
             tot.draws += c.draws; tot.nscatt += c.nscatt;
             for (int i = 0; i < 24; ++i) tot.mom[i] += c.mom[i];
+            for (int i = 0; i < 3 * kAdjGroups; ++i) tot.adj[i] += c.adj[i];
+            tot.loss += c.loss;
         }
+    }
+    if (adj_out && A.adj) {  // [d/d mua of groups..., d/d mus..., d/d g...], then L
+        const int G = A.adj->ngroups;
+        for (int k = 0; k < 3; ++k)
+            for (int gi = 0; gi < G; ++gi) adj_out[k * G + gi] = tot.adj[k * kAdjGroups + gi];
+        adj_out[3 * G] = tot.loss;
     }
     if (st) {
         std::memset(st, 0, sizeof(*st));
@@ -1316,6 +1412,45 @@ int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt
     else run_all<double>(A, stats, threads);
     if (jmean && pol->tally_f32)
         for (int64_t i = 0; i < ncell; ++i) jmean[i] = (double)j32[i];
+    return SMCRT_OK;
+}
+
+int32_t oracle_adjoint(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* src,
+                       const smcrt_detector* dets, int32_t ndet, const oracle_policy* pol, int64_t nphotons,
+                       uint64_t seed, const double* w, const double* h, const int32_t* region_group,
+                       int32_t ngroups, double* grad) {
+    if (validate_scene(scene) || !grid || !src || !pol || !w || !region_group || !grad || nphotons < 0 ||
+        ngroups < 1 || ngroups > kAdjGroups || (ndet > 0 && !dets))
+        return SMCRT_ERR_ARG;
+    if (grid->nxg <= 0 || grid->nyg <= 0 || grid->nzg <= 0) return SMCRT_ERR_ARG;
+    for (int r = 0; r < scene->nregions; ++r)
+        if (region_group[r] < -1 || region_group[r] >= ngroups) return SMCRT_ERR_ARG;
+    RunArgs A{};
+    A.scene = scene;
+    A.grid = grid;
+    A.src = src;
+    int64_t nbins = 0;
+    if (ndet > 0) A.dets = make_dets(dets, ndet, nbins);
+    for (const Det& D : A.dets)
+        if (D.d.layer < 1 || D.d.layer > scene->nregions) return SMCRT_ERR_ARG;
+    A.kernel = SMCRT_KERNEL_PATHLENGTH;
+    A.pol.eps = pol->eps;
+    A.pol.delta = pol->delta;
+    A.pol.h = pol->normal_h;
+    A.pol.ref_dda = pol->ref_dda != 0;
+    A.pol.crossing_f64 = pol->crossing_f64 != 0;
+    A.pol.kill_le = pol->ref_dda == 0;
+    A.pol.max_steps = pol->max_trace_steps > 0 ? pol->max_trace_steps : 1000000;
+    A.first = 0;
+    A.count = nphotons;
+    A.seed = seed;
+    std::vector<double> binbuf(std::max<int64_t>(nbins, 1), 0.0);
+    A.bins = binbuf.data();
+    AdjArgs adj{w, h, region_group, ngroups};
+    A.adj = &adj;
+    const int threads = pol->threads > 0 ? pol->threads : oracle_max_threads();
+    if (pol->precision == SMCRT_FP32) run_all<float>(A, nullptr, threads, grad);
+    else run_all<double>(A, nullptr, threads, grad);
     return SMCRT_OK;
 }
 

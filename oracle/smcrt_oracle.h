@@ -40,6 +40,18 @@ int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt
 
 int64_t oracle_detector_bins(const smcrt_detector* dets, int32_t ndet);
 
+/* Perturbation Monte Carlo (likelihood-ratio) reference gradient of
+ * L = sum_v w[v] jmean[v] + sum_b h[b] bins[b] over packets [0, nphotons) of the
+ * pathlength kernel (src/kernelsMod.f90:265-321) with respect to each region
+ * group's (mua, mus, g): the sum over packets of C * d log p(path), C the packet's
+ * contribution to L.  w: nxg*nyg*nzg voxel weights; h: detector bin weights or
+ * NULL; region_group[r] in -1..ngroups-1 (ngroups <= 16).  grad: 3*ngroups + 1
+ * doubles, [d/d mua..., d/d mus..., d/d g..., L]. */
+int32_t oracle_adjoint(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* src,
+                       const smcrt_detector* dets, int32_t ndet, const oracle_policy* pol,
+                       int64_t nphotons, uint64_t seed, const double* w, const double* h,
+                       const int32_t* region_group, int32_t ngroups, double* grad);
+
 int32_t oracle_eval_sdf(const smcrt_scene* scene, int32_t precision, const double* pts,
                         int64_t npts, double* out);
 /* render_sub (src/sdfs/sdf_base.f90:302-346): min over regions at every voxel,
