@@ -1,0 +1,68 @@
+"""The host mirror on the reference's own input files (res/*.toml of signedMCRT),
+read in place: each parses, or fails, as the reference's parser does, and each
+scene the reference can build is built here with the same number of SDF regions.
+
+Failures that are the reference's own: exp.toml and slab_test.toml give an annulus
+and a dslit source no `position`, which get_vector rejects
+(src/parse/parse_helpers.f90:44-51, called from src/parse/parse_source.f90:61);
+skin.toml gives a uniform source no point1 (parse_source.f90:126-131); jacques,
+lens, neural and raman_test are not in setup_simulation's switch
+(src/setup.f90:33-51, "no such routine").  logo and vessels need an SVG include or
+external vessel files, which this transport does not model.
+"""
+import os
+from pathlib import Path
+
+import pytest
+
+from signedmcrt_b200 import presets as P
+from signedmcrt_b200.config import ConfigError, parse_params
+from signedmcrt_b200.scene import FlatScene
+
+RES = Path(os.environ.get("SMCRT_REFERENCE_ROOT", "/root/reference")) / "res"
+
+# file -> ("ok", geom_name, regions) | ("parse", message) | ("scene", message)
+EXPECTED = {
+    "aptran.toml": ("ok", "aptran", 3),
+    "input.toml": ("ok", "test_egg", 4),
+    "omg.toml": ("ok", "omg", 2),
+    "scat_test.toml": ("ok", "scat_test", 2),
+    "scat_test2.toml": ("ok", "scat_test2", 1),
+    "sphere.toml": ("ok", "sphere_scene", 41),
+    "test_dects.toml": ("ok", "scat_test", 2),
+    "test_spectra_1D.toml": ("ok", "scat_test", 2),
+    "test_spectra_2D.toml": ("ok", "scat_test", 2),
+    "test_spectra_const.toml": ("ok", "scat_test", 2),
+    "exp.toml": ("parse", "Expected vector of size 3 for position"),
+    "slab_test.toml": ("parse", "Expected vector of size 3 for position"),
+    "skin.toml": ("parse", "Uniform source requires point1 variable"),
+    "jacques.toml": ("scene", "no such routine"),
+    "lens.toml": ("scene", "no such routine"),
+    "neural.toml": ("scene", "no such routine"),
+    "raman.toml": ("scene", "no such routine"),
+    "logo.toml": ("scene", "svg include"),
+    "vessels.toml": ("scene", "svg include"),
+}
+
+pytestmark = pytest.mark.skipif(not RES.is_dir(), reason="the reference's res/ directory is not present")
+
+
+def test_every_reference_input_is_listed():
+    assert sorted(p.name for p in RES.glob("*.toml")) == sorted(EXPECTED)
+
+
+@pytest.mark.parametrize("name", sorted(EXPECTED))
+def test_reference_input(name):
+    kind, *rest = EXPECTED[name]
+    if kind == "parse":
+        with pytest.raises(ConfigError, match=rest[0]):
+            parse_params(RES / name)
+        return
+    st = parse_params(RES / name)
+    if kind == "scene":
+        with pytest.raises(ConfigError, match=rest[0]):
+            P.setup_simulation(st)
+        return
+    geom, regions = rest
+    assert st.geometry.geom_name == geom
+    assert FlatScene(P.setup_simulation(st)).nregions == regions
