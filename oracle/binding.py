@@ -68,6 +68,10 @@ def lib() -> C.CDLL:
                                 C.c_int64, C.c_uint64, P(C.c_double), P(C.c_double), P(C.c_int32), C.c_int32,
                                 P(C.c_double)], C.c_int32),
             "oracle_eval_sdf": ([P(abi.Scene), C.c_int32, P(C.c_double), C.c_int64, P(C.c_double)], C.c_int32),
+            "oracle_intersect_plane": ([P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double)],
+                                       C.c_int32),
+            "oracle_intersect_circle": ([P(C.c_double), P(C.c_double), C.c_double, P(C.c_double), P(C.c_double),
+                                        P(C.c_double)], C.c_int32),
             "oracle_calc_normal": ([P(abi.Scene), C.c_int32, C.c_double, P(C.c_double), C.c_int64,
                                     P(C.c_double)], C.c_int32),
             "oracle_render": ([P(abi.Scene), C.c_int32, P(C.c_int32), P(C.c_double), P(C.c_float)], C.c_int32),
@@ -174,6 +178,26 @@ def render(flat: FlatScene, samples, extent, precision: str = "fp64") -> np.ndar
                                ns.ctypes.data_as(C.POINTER(C.c_int32)), abi.dptr(ext),
                                img.ctypes.data_as(C.POINTER(C.c_float))) == 0
     return img.reshape(tuple(int(x) for x in ns), order="F")
+
+
+def _v3(v):
+    return np.ascontiguousarray(v, dtype=np.float64)
+
+
+def intersect_plane(n, p0, l0, l) -> tuple[bool, float]:
+    """intersectPlane (src/geometryMod.f90:217-241): (hit, t)."""
+    t = C.c_double(0.0)
+    hit = lib().oracle_intersect_plane(abi.dptr(_v3(n)), abi.dptr(_v3(p0)), abi.dptr(_v3(l0)), abi.dptr(_v3(l)),
+                                       C.byref(t))
+    return bool(hit), t.value
+
+
+def intersect_circle(n, p0, radius, l0, l) -> tuple[bool, float]:
+    """intersectCircle (src/geometryMod.f90:244-270): (hit, t)."""
+    t = C.c_double(0.0)
+    hit = lib().oracle_intersect_circle(abi.dptr(_v3(n)), abi.dptr(_v3(p0)), float(radius), abi.dptr(_v3(l0)),
+                                        abi.dptr(_v3(l)), C.byref(t))
+    return bool(hit), t.value
 
 
 def calc_normal(flat: FlatScene, region0: int, pts, h: float = 1e-6) -> np.ndarray:

@@ -1027,6 +1027,25 @@ std::vector<Det> make_dets(const smcrt_detector* dets, int ndet, int64_t& total)
 inline int64_t nint_(double x) { return (int64_t)std::llround(x); }  // Fortran nint: half away from zero
 
 // returns global bin or -1
+// intersectPlane, src/geometryMod.f90:217-241: the ray l0 + t l meets the plane
+// through p0 with normal n from its front side (n . l > 1e-6) at t >= 0.
+inline bool intersect_plane(const double n[3], const double p0[3], const double l0[3], const double l[3],
+                            double& t) {
+    const double denom = n[0] * l[0] + n[1] * l[1] + n[2] * l[2];
+    if (!(denom > 1e-6)) return false;
+    t = ((p0[0] - l0[0]) * n[0] + (p0[1] - l0[1]) * n[1] + (p0[2] - l0[2]) * n[2]) / denom;
+    return t >= 0.0;
+}
+
+// intersectCircle, src/geometryMod.f90:244-270: the plane hit lies within radius of p0.
+inline bool intersect_circle(const double n[3], const double p0[3], double radius, const double l0[3],
+                             const double l[3], double& t) {
+    t = 0.0;
+    if (!intersect_plane(n, p0, l0, l, t)) return false;
+    const double q[3] = {l0[0] + l[0] * t - p0[0], l0[1] + l[1] * t - p0[1], l0[2] + l[2] * t - p0[2]};
+    return std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) <= radius;
+}
+
 int64_t det_bin(const Det& D, const double p[3], const double l[3], double value, int layer1) {
     const smcrt_detector& d = D.d;
     if (d.layer != layer1) return -1;
@@ -1035,12 +1054,8 @@ int64_t det_bin(const Det& D, const double p[3], const double l[3], double value
                              (p[2] - d.pos[2]) * (p[2] - d.pos[2]));
         if (!(r >= d.r1 && r <= d.r2)) return -1;
     } else if (d.kind == SMCRT_DET_CIRCLE) {
-        double denom = d.dir[0] * l[0] + d.dir[1] * l[1] + d.dir[2] * l[2];
-        if (!(denom > 1e-6)) return -1;
-        double t = ((d.pos[0] - p[0]) * d.dir[0] + (d.pos[1] - p[1]) * d.dir[1] + (d.pos[2] - p[2]) * d.dir[2]) / denom;
-        if (!(t >= 0)) return -1;
-        double q[3] = {p[0] + l[0] * t - d.pos[0], p[1] + l[1] * t - d.pos[1], p[2] + l[2] * t - d.pos[2]};
-        if (!(std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) <= d.r1)) return -1;
+        double t;
+        if (!intersect_circle(d.dir, d.pos, d.r1, p, l, t)) return -1;
         if (t > 5e-3) return -1;
     } else {  // camera
         double num = (d.pos[0] - p[0]) * D.n[0] + (d.pos[1] - p[1]) * D.n[1] + (d.pos[2] - p[2]) * D.n[2];
@@ -1452,6 +1467,21 @@ int32_t oracle_adjoint(const smcrt_scene* scene, const smcrt_grid* grid, const s
     if (pol->precision == SMCRT_FP32) run_all<float>(A, nullptr, threads, grad);
     else run_all<double>(A, nullptr, threads, grad);
     return SMCRT_OK;
+}
+
+int32_t oracle_intersect_plane(const double* n, const double* p0, const double* l0, const double* l, double* t) {
+    double tt = 0.0;
+    const bool hit = intersect_plane(n, p0, l0, l, tt);
+    if (t) *t = tt;
+    return hit ? 1 : 0;
+}
+
+int32_t oracle_intersect_circle(const double* n, const double* p0, double radius, const double* l0, const double* l,
+                                double* t) {
+    double tt = 0.0;
+    const bool hit = intersect_circle(n, p0, radius, l0, l, tt);
+    if (t) *t = tt;
+    return hit ? 1 : 0;
 }
 
 int32_t oracle_eval_sdf(const smcrt_scene* scene, int32_t precision, const double* pts, int64_t npts, double* out) {

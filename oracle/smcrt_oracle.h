@@ -52,6 +52,13 @@ int32_t oracle_adjoint(const smcrt_scene* scene, const smcrt_grid* grid, const s
                        int64_t nphotons, uint64_t seed, const double* w, const double* h,
                        const int32_t* region_group, int32_t ngroups, double* grad);
 
+/* intersectPlane / intersectCircle (src/geometryMod.f90:217-270), the geometry of
+ * the circle detector: 1 on a hit, 0 otherwise; *t the ray parameter. */
+int32_t oracle_intersect_plane(const double* n, const double* p0, const double* l0, const double* l,
+                               double* t);
+int32_t oracle_intersect_circle(const double* n, const double* p0, double radius, const double* l0,
+                                const double* l, double* t);
+
 int32_t oracle_eval_sdf(const smcrt_scene* scene, int32_t precision, const double* pts,
                         int64_t npts, double* out);
 /* render_sub (src/sdfs/sdf_base.f90:302-346): min over regions at every voxel,

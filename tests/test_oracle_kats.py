@@ -306,3 +306,20 @@ def test_render_matches_restatement(oracle, scene, precision):
         want = _render_restated(oracle, flat, samples, (2.0, 1.5, 1.0), precision)
         got = oracle.render(flat, samples, (2.0, 1.5, 1.0), precision)
         np.testing.assert_array_equal(got, want)
+
+
+def test_intersection_known_answers(oracle):
+    """test/geometry/test_geometry.f90 test_plane and test_circle: a ray from
+    (0,0,-10) along +z meets the z = 0 plane (and the r = 10 disc) at the origin; a
+    ray from (0,0,-20) along -z meets neither.  These are the circle detector's hit
+    test (check_hit_circle, src/detectors/detectors.f90:110-127)."""
+    n, c = (0.0, 0.0, 1.0), (0.0, 0.0, 0.0)
+    for hit_fn in (lambda o, d: oracle.intersect_plane(n, c, o, d),
+                   lambda o, d: oracle.intersect_circle(n, c, 10.0, o, d)):
+        hit, t = hit_fn((0.0, 0.0, -10.0), (0.0, 0.0, 1.0))
+        assert hit and np.allclose(np.array([0.0, 0.0, -10.0]) + t * np.array([0.0, 0.0, 1.0]), 0.0)
+        hit, _ = hit_fn((0.0, 0.0, -20.0), (0.0, 0.0, -1.0))
+        assert not hit
+    # beyond the radius the plane is hit but the disc is not
+    assert oracle.intersect_plane(n, c, (11.0, 0.0, -1.0), (0.0, 0.0, 1.0))[0]
+    assert not oracle.intersect_circle(n, c, 10.0, (11.0, 0.0, -1.0), (0.0, 0.0, 1.0))[0]
