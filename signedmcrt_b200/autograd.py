@@ -24,12 +24,15 @@ class _Transport(torch.autograd.Function):
     @staticmethod
     def forward(ctx, params, scene_fn, settings, region_group, nphotons, seed):
         optics = params.detach().cpu().numpy().astype(np.float64)
-        tr = Transport(scene_fn(optics), settings, kernel="pathlength", precision="fp32")
         dev = torch.device("cuda")
+        # the transport runs on torch's current stream, so it follows the zero-fills
+        # below and precedes the ops that read the tallies
+        stream = torch.cuda.current_stream(dev)
+        tr = Transport(scene_fn(optics), settings, kernel="pathlength", precision="fp32",
+                       stream=stream.cuda_stream)
         jm = torch.zeros(tr.ncell, dtype=torch.float64, device=dev)
         bins = torch.zeros(max(tr.nbins, 1), dtype=torch.float64, device=dev)
         tr.run_device(0, int(nphotons), int(seed), jm.data_ptr(), bins.data_ptr() if tr.nbins else None)
-        torch.cuda.synchronize()
         nx, ny, nz = tr.shape
         phi = (jm / nphotons).reshape(nz, ny, nx).permute(2, 1, 0)
         det = bins[: tr.nbins] / nphotons
@@ -49,6 +52,9 @@ class _Transport(torch.autograd.Function):
         gb = None
         if grad_det is not None and tr.nbins:
             gb = grad_det.to(torch.float64).contiguous()
+        # the adjoint launches on the forward's stream: the weights made on the
+        # backward's current stream must be complete first
+        torch.cuda.current_stream(w.device).synchronize()
         grad, _ = tr.adjoint(ctx.n, ctx.seed, w.data_ptr(), gb.data_ptr() if gb is not None else None,
                              ctx.region_group, ctx.ngroups)
         tr.close()

@@ -6,7 +6,10 @@ Each one does what the Fortran routine does around its packet loop -- parse the
 TOML input (`setup`, :453-546), run every packet, then `finalise` (:548-633):
 print the mean number of scatters, normalise the fluence, write
 `data/jmean/<output.fluence>` with the run's metadata and the detector files.
-The packet loop itself is the GPU kernel behind the C ABI.
+Like the reference's serial build, `nscatt.dat` (mean scatters per packet,
+:596-599) goes to the working directory, and `test_kernel` writes
+`positions.dat` there too (:439-446): the files the reference's end-to-end
+tests read.  The packet loop itself is the GPU kernel behind the C ABI.
 
 Checkpoints (`[simulation] checkpoint_every_n`, `checkpoint_file`) are written in
 the reference's layout every `checkpoint_every_n` packets, with the FP64 tally
@@ -108,6 +111,11 @@ def run_kernel(settings: Settings, kernel: str, *, end_early: bool = False, inpu
         files.append(writer.write_data(fluence, base / "jmean" / st.output.fluence, st.output.overwrite, meta))
         if st.detectors:
             files += writer.write_detected_photons(st, bins, base / "detectors")
+        cwd = Path(root) if root is not None else Path.cwd()
+        if np.isfinite(nscatt):
+            files.append(writer.write_nscatt(nscatt, nphotons, cwd / "nscatt.dat"))
+        if kernel == "test":
+            files.append(writer.write_positions(stats["moments"], nphotons, cwd / "positions.dat"))
     return KernelRun(jmean, fluence, bins, nscatt, stats, files)
 
 

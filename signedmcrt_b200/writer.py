@@ -222,3 +222,31 @@ def load_checkpoint(filename: str | Path, shape, dtype=None) -> tuple[str, int, 
     dt = np.dtype(dtype)
     arr = np.frombuffer(raw[l2 + 1:l2 + 1 + n * dt.itemsize], dtype=dt).reshape(shape, order="F")
     return toml, nrun, arr
+
+
+def write_positions(moments, nphotons: int, filename: str | Path = "positions.dat") -> Path:
+    """positions.dat of test_kernel (src/kernelsMod.f90:439-446): 8 lines of x y z,
+    the 1st moments of the positions of scatter events 1-4 times 10 / nphotons,
+    then their 2nd moments times 100 / nphotons (mean-free-path units of the
+    Scatter_test2 table).  `moments` is the 24 sums of the test kernel: sum of
+    positions (4 x 3) then sum of squared positions (4 x 3)."""
+    m = np.asarray(moments, dtype=np.float64).reshape(2, 4, 3)
+    n = float(nphotons)
+    rows = [10.0 * m[0, i] / n for i in range(4)] + [100.0 * m[1, i] / n for i in range(4)]
+    p = Path(filename)
+    p.write_text("".join(" ".join(f"{v:.17g}" for v in r) + "\n" for r in rows))
+    return p
+
+
+def write_nscatt(nscatt: float, nphotons: int, filename: str | Path = "nscatt.dat") -> Path:
+    """nscatt.dat of finalise (src/kernelsMod.f90:596-599): the mean number of
+    scatters per packet, read back by Scatter_test1."""
+    p = Path(filename)
+    p.write_text(f"{float(nscatt) / float(nphotons):.17g}\n")
+    return p
+
+
+def read_table(filename: str | Path) -> np.ndarray:
+    """The whitespace-separated numbers of positions.dat / nscatt.dat, one row per line."""
+    return np.array([[float(x) for x in line.split()] for line in Path(filename).read_text().splitlines()
+                     if line.strip()])

@@ -75,3 +75,16 @@ def test_checkpoint_round_trip(tmp_path, dtype):
     toml, nrun, b = W.load_checkpoint(p, a.shape)
     assert toml == "in.toml" and nrun == 12345 and b.dtype == dtype
     np.testing.assert_array_equal(b, a.astype(dtype))
+
+
+def test_positions_and_nscatt_files(tmp_path):
+    """positions.dat (src/kernelsMod.f90:439-446): 8 rows, first moments x 10 / N then
+    second moments x 100 / N; nscatt.dat (:596-599): mean scatters per packet."""
+    m = np.arange(24, dtype=np.float64)
+    p = W.write_positions(m, 1000, tmp_path / "positions.dat")
+    rows = W.read_table(p)
+    assert rows.shape == (8, 3)
+    np.testing.assert_allclose(rows[:4], 10.0 * m[:12].reshape(4, 3) / 1000, rtol=1e-15)
+    np.testing.assert_allclose(rows[4:], 100.0 * m[12:].reshape(4, 3) / 1000, rtol=1e-15)
+    q = W.write_nscatt(5750000.0, 100000, tmp_path / "nscatt.dat")
+    assert W.read_table(q)[0, 0] == 57.5
