@@ -23,7 +23,7 @@ LIB_PATH = HERE / "lib" / "libsmcrt_oracle.so"
 
 class Policy(C.Structure):
     _fields_ = [("precision", C.c_int32), ("ref_dda", C.c_int32), ("crossing_f64", C.c_int32),
-                ("tally_f32", C.c_int32), ("threads", C.c_int32), ("reserved", C.c_int32),
+                ("tally_f32", C.c_int32), ("threads", C.c_int32), ("near_surface_f64", C.c_int32),
                 ("eps", C.c_double), ("delta", C.c_double), ("normal_h", C.c_double),
                 ("max_trace_steps", C.c_int64)]
 
@@ -34,14 +34,16 @@ def reference_policy(threads: int = 0, tally_f32: bool = False) -> Policy:
 
 
 def device_policy(precision: str, grid: abi.Grid, threads: int = 0) -> Policy:
-    """The GPU algorithm: integer voxel walk, FP64 boundary events, default epsilon."""
+    """The GPU algorithm: integer voxel walk, FP64 boundary events, default epsilon;
+    in FP32, sweeps within 2 eps of a surface and after crossing steps in FP64."""
     if precision == "fp64":
         eps = 1e-8
     else:
         L = max(grid.xmax, grid.ymax, grid.zmax)
         m, e = np.frexp(L)
         eps = max(1e-8, 8.0 * np.ldexp(1.0, int(e) - 24))
-    return Policy(abi.FP32 if precision == "fp32" else abi.FP64, 0, 1, 0, threads, 0, eps, 1e-8, 1e-6, 0)
+    near = 1 if precision == "fp32" else 0
+    return Policy(abi.FP32 if precision == "fp32" else abi.FP64, 0, 1, 0, threads, near, eps, 1e-8, 1e-6, 0)
 
 
 _lib = None

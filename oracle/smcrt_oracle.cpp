@@ -464,6 +464,7 @@ struct Pol {
     double eps, delta, h;
     bool ref_dda, crossing_f64;
     bool kill_le;  // device semantics: d <= eps at the start of a flight counts as on the surface
+    bool near_f64; // device FP32 semantics: near-surface and crossing sweeps in FP64 (see sweep)
     int64_t max_steps;
 };
 
@@ -606,6 +607,61 @@ inline V3<double> advance(V3<double> p, R d, V3<R> dir) {
 }
 
 // ---------------------------------------------------------------------------
+// One sweep of every region at a point (the N evaluations of inttau2.f90:52-56,
+// 86-90, 104-108, 117-121 and kernelsMod.f90:275-280): the values in transport
+// precision R, their signed minimum, minimum |d|, the first region containing the
+// point (-1: none) and the innermost containing region (the launch layer; 0 when
+// none contains it).  Device FP32 semantics (pol.near_f64), as the GPU's FP32
+// kernels do it: a sweep whose FP32 minimum |d| is within 2 eps of a surface, and
+// every sweep after a crossing step (force64), is taken instead in FP64 at the
+// FP64 position with the FP64 scene; its values are rounded to R and its region
+// indices come from the FP64 values.
+template <class R>
+struct SweepRes {
+    R mn, mna;
+    int nl, lay;
+};
+template <class T>
+void sweep_stats(const T* v, int N, T& mn, T& mna, int& nl, int& lay) {
+    mn = mna = std::numeric_limits<T>::infinity();
+    nl = -1;
+    lay = 0;
+    T inner = std::numeric_limits<T>::infinity();
+    for (int i = 0; i < N; ++i) {
+        const T d = v[i];
+        mn = std::min(mn, d);
+        mna = std::min(mna, std::fabs(d));
+        if (nl < 0 && d < (T)0) nl = i;
+        const T a = (d > (T)0) ? (T)999.0 : std::fabs(d);
+        if (a < inner) {
+            inner = a;
+            lay = i;
+        }
+    }
+}
+template <class R>
+SweepRes<R> sweep(const Scene<R>& sc, const Scene<double>& sc64, const Pol& pol, V3<double> pos, bool force64,
+                  R* out) {
+    const int N = (int)sc.regions.size();
+    SweepRes<R> o;
+    if (!(pol.near_f64 && force64)) {
+        const V3<R> p = cv<R>(pos);
+        for (int i = 0; i < N; ++i) out[i] = eval_region(sc, i, p);
+        sweep_stats(out, N, o.mn, o.mna, o.nl, o.lay);
+        if (!pol.near_f64 || sizeof(R) == 8 || o.mna > (R)2 * (R)pol.eps) return o;
+    }
+    thread_local std::vector<double> v64;
+    v64.resize(N);
+    for (int i = 0; i < N; ++i) v64[i] = eval_region(sc64, i, pos);
+    double mn, mna;
+    sweep_stats(v64.data(), N, mn, mna, o.nl, o.lay);
+    for (int i = 0; i < N; ++i) out[i] = (R)v64[i];
+    o.mn = (R)mn;
+    o.mna = (R)mna;
+    return o;
+}
+
+// ---------------------------------------------------------------------------
 // Boundary event: normal (calcNormal) + reflect_refract in precision E.
 template <class R, class E, class Rng>
 bool boundary_event(const Scene<E>& scE, int which, int L, int nl, V3<double> pos, V3<R>& dir, R h, Rng& rng,
@@ -650,8 +706,9 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
     }
     bool ok = true;
     for (;;) {
-        R dsdf = std::numeric_limits<R>::infinity();
-        for (int i = 0; i < N; ++i) dsdf = std::min(dsdf, std::fabs(eval_region(sc, i, cv<R>(pos))));
+        // dstmp holds the values of the latest sweep: at a surface they are the
+        // reference's dstmp sweep (:104-108), taken at the same point
+        R dsdf = sweep(sc, sc64, pol, pos, false, dstmp.data()).mna;
         c.sdf += N;
         // reference: kill if d < eps (inttau2.f90:58); device semantics also kills
         // at d == eps, where the trace loop (d > eps, :63) has already stopped
@@ -683,16 +740,10 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
                 break;
             }
             if (!ok) break;
-            R mn = std::numeric_limits<R>::infinity(), mna = mn;
-            const V3<R> pf = cv<R>(pos);
-            for (int i = 0; i < N; ++i) {
-                R d = eval_region(sc, i, pf);
-                mn = std::min(mn, d);
-                mna = std::min(mna, std::fabs(d));
-            }
+            const SweepRes<R> sw = sweep(sc, sc64, pol, pos, false, dstmp.data());
             c.sdf += N;
-            dsdf = mna;
-            if (mn >= (R)0) {
+            dsdf = sw.mna;
+            if (sw.mn >= (R)0) {
                 pk.tflag = true;
                 break;
             }
@@ -712,21 +763,12 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
         if (taurun >= tau || pk.tflag) break;
 
         R mind = std::numeric_limits<R>::infinity();
-        const V3<R> pf0 = cv<R>(pos);
-        for (int i = 0; i < N; ++i) {
-            dstmp[i] = eval_region(sc, i, pf0);
-            mind = std::min(mind, std::fabs(dstmp[i]));
-        }
+        for (int i = 0; i < N; ++i) mind = std::min(mind, std::fabs(dstmp[i]));
         c.sdf += N;
         R dstep = mind + (R)2 * eps;
         oldpos = pos;
         pos = advance(pos, dstep, dir);
-        int nl = -1;
-        const V3<R> pf1 = cv<R>(pos);
-        for (int i = 0; i < N; ++i) {
-            ds[i] = eval_region(sc, i, pf1);
-            if (nl < 0 && ds[i] < (R)0) nl = i;
-        }
+        int nl = sweep(sc, sc64, pol, pos, true, ds.data()).nl;
         c.sdf += N;
         if (nl < 0) nl = 0;  // minloc of an all-zero array
         const int L = pk.layer;
@@ -964,19 +1006,11 @@ void emit(const smcrt_source& s, const GridD& g, Packet<R>& pk, Rng& rng) {
 
 // Launch layer: innermost containing region (src/kernelsMod.f90:275-280).
 template <class R>
-int launch_layer(const Scene<R>& sc, V3<R> p, Counters& c) {
-    int best = 0;
-    R bestv = std::numeric_limits<R>::infinity();
-    for (int i = 0; i < (int)sc.regions.size(); ++i) {
-        R d = eval_region(sc, i, p);
-        if (d > (R)0) d = (R)(-999.0);
-        if (std::fabs(d) < bestv) {
-            bestv = std::fabs(d);
-            best = i;
-        }
-    }
+int launch_layer(const Scene<R>& sc, const Scene<double>& sc64, const Pol& pol, V3<double> p, Counters& c) {
+    thread_local std::vector<R> v;
+    v.resize(sc.regions.size());
     c.sdf += sc.regions.size();
-    return best;
+    return sweep(sc, sc64, pol, p, false, v.data()).lay;
 }
 
 // ---------------------------------------------------------------------------
@@ -1156,7 +1190,7 @@ void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, c
         }
     };
     emit(*A.src, g, pk, rng);
-    pk.layer = launch_layer(sc, cv<R>(pk.pos), c);
+    pk.layer = launch_layer(sc, sc64, A.pol, pk.pos, c);
     tauint2(sc, sc64, g, A.pol, pk, rng, t, c, lp, adj ? &by_tau : nullptr);
     if (adj) flights();
     if (A.kernel == SMCRT_KERNEL_WEIGHT) {  // weight_scatter :99-134
@@ -1395,6 +1429,7 @@ int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt
     A.pol.ref_dda = pol->ref_dda != 0;
     A.pol.crossing_f64 = pol->crossing_f64 != 0;
     A.pol.kill_le = pol->ref_dda == 0;  // device semantics
+    A.pol.near_f64 = pol->near_surface_f64 != 0;
     A.pol.max_steps = pol->max_trace_steps > 0 ? pol->max_trace_steps : 1000000;
     A.first = first;
     A.count = count;
@@ -1455,6 +1490,7 @@ int32_t oracle_adjoint(const smcrt_scene* scene, const smcrt_grid* grid, const s
     A.pol.ref_dda = pol->ref_dda != 0;
     A.pol.crossing_f64 = pol->crossing_f64 != 0;
     A.pol.kill_le = pol->ref_dda == 0;
+    A.pol.near_f64 = pol->near_surface_f64 != 0;
     A.pol.max_steps = pol->max_trace_steps > 0 ? pol->max_trace_steps : 1000000;
     A.first = 0;
     A.count = nphotons;
@@ -1580,21 +1616,30 @@ int32_t oracle_emit(const smcrt_scene* scene, const smcrt_grid* grid, const smcr
     if (validate_scene(scene) || !grid || !src) return SMCRT_ERR_ARG;
     GridD g(*grid);
     Counters c;
+    // the launch layer as the transport kernels take it: FP32 with the
+    // near-surface FP64 rule and the FP32 default epsilon, or FP64
+    Pol pol{};
+    pol.near_f64 = precision == SMCRT_FP32;
+    {
+        int e;
+        std::frexp(std::max(grid->xmax, std::max(grid->ymax, grid->zmax)), &e);
+        pol.eps = precision == SMCRT_FP32 ? std::max(1e-8, 8.0 * std::ldexp(1.0, e - 24)) : 1e-8;
+    }
+    const Scene<double> sc64 = make_scene<double>(scene);
     for (int64_t q = 0; q < npk; ++q) {
         if (precision == SMCRT_FP32) {
             Scene<float> sc = make_scene<float>(scene);
             PhiloxStream<float> rng(seed, 0, (uint64_t)(first + q));
             Packet<float> pk{};
             emit(*src, g, pk, rng);
-            layer[q] = launch_layer(sc, cv<float>(pk.pos), c) + 1;
+            layer[q] = launch_layer(sc, sc64, pol, pk.pos, c) + 1;
             pos[3 * q] = pk.pos.x; pos[3 * q + 1] = pk.pos.y; pos[3 * q + 2] = pk.pos.z;
             dir[3 * q] = pk.dir.x; dir[3 * q + 1] = pk.dir.y; dir[3 * q + 2] = pk.dir.z;
         } else {
-            Scene<double> sc = make_scene<double>(scene);
             PhiloxStream<double> rng(seed, 0, (uint64_t)(first + q));
             Packet<double> pk{};
             emit(*src, g, pk, rng);
-            layer[q] = launch_layer(sc, cv<double>(pk.pos), c) + 1;
+            layer[q] = launch_layer(sc64, sc64, pol, pk.pos, c) + 1;
             pos[3 * q] = pk.pos.x; pos[3 * q + 1] = pk.pos.y; pos[3 * q + 2] = pk.pos.z;
             dir[3 * q] = pk.dir.x; dir[3 * q + 1] = pk.dir.y; dir[3 * q + 2] = pk.dir.z;
         }

@@ -24,7 +24,8 @@ typedef struct oracle_policy {
     int32_t crossing_f64;   /* 1: normal + Fresnel + reflect/refract in FP64 (the GPU's FP32 path) */
     int32_t tally_f32;      /* 1: accumulate jmean in FP32 like the reference (iarray.f90:12) */
     int32_t threads;        /* OpenMP threads; 0 = all */
-    int32_t reserved;
+    int32_t near_surface_f64;/* 1: the GPU's FP32 kernels' rule -- a sweep within 2 eps of a
+                               surface, and every sweep after a crossing step, in FP64 */
     double eps;             /* surface epsilon (reference 1e-8) */
     double delta;           /* voxel snap (reference 1e-8, inttau2.f90:239) */
     double normal_h;        /* calcNormal step (reference 1e-6) */
