@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define SMCRT_ABI_VERSION 2
+#define SMCRT_ABI_VERSION 3
 
 /* ---- status codes -------------------------------------------------------- */
 enum smcrt_status {
@@ -197,6 +197,13 @@ typedef struct smcrt_options {
                               tally): 0 = library choice (as many as fit in
                               64 MiB, at most 8), 1 = a single grid, up to 16;
                               rounded down to a power of two */
+    int32_t scene_memory;  /* where the kernel reads the scene: 0 = the launch's
+                              parameter block when the scene fits (at most 16
+                              regions and 32 primitives), device memory otherwise
+                              (up to 255 regions and 4096 primitives, with a
+                              bounding-sphere cull of the SDF sweep); 1 = device
+                              memory always */
+    int32_t reserved[7];   /* zero */
 } smcrt_options;
 
 /* Event counters of one run (definitions identical in the CPU oracle). */
@@ -217,6 +224,12 @@ typedef struct smcrt_stats {
     double kernel_ms;            /* device time of the transport kernel(s) */
     int32_t device_status;       /* 0 or a bitmask of device status flags */
     int32_t reserved;
+    uint64_t h2d_bytes;          /* host-to-device bytes the call moved: the launch's kernel
+                                    parameter block (scene, grid, source, detectors, run
+                                    settings) and any uploaded tables */
+    uint64_t d2h_bytes;          /* device-to-host bytes the call moved: tallies copied to
+                                    host buffers and the event counters */
+    uint64_t reserved2[6];
 } smcrt_stats;
 
 /* Per-packet final state (history replay). */
@@ -353,19 +366,27 @@ int32_t smcrt_run_batched(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* 
                           const uint64_t* seeds, double* const* jmeans,
                           double* const* det_bins, smcrt_stats* stats);
 
-/* Allocation-free form of smcrt_run_device, for callers that cannot allocate
- * device memory (inside a CUDA stream capture, under an application-owned memory
- * pool, or with device memory budgeted up front).  It takes the same inputs as
- * smcrt_create plus caller-owned DEVICE tally buffers, creates no context, and
+/* Allocation-free form of smcrt_run_device (no counterpart in the reference,
+ * where signedMCRT allocates its tallies itself).  It is for callers that cannot
+ * let a library allocate device memory: applications that hand out every byte of
+ * device memory from their own pool allocator, or processes whose device memory
+ * is reserved up front for a fixed budget.  It takes the same inputs as
+ * smcrt_create plus caller-owned DEVICE tally buffers, creates no context and
  * calls no cudaMalloc/cudaFree: the kernel's scratch (work counter, event
- * counters, status) is a static device array of smcrt_static_scratch_bytes()
- * bytes inside the library, present on every GPU that loads it until exit.
- * ADDS the tallies of packets [first, first+count) into jmean_dev/det_bins_dev
- * on opts->stream (NULL = default stream).  The first call on a device resolves
- * the array's device address; make that first call before any stream capture.
- * All calls share the one array: calls that overlap on the GPU race on it.
- * If stats is not NULL the call synchronises the stream and fills it.
- * No counterpart in the reference (signedMCRT allocates its tallies itself). */
+ * counters, status word; about 300 bytes) lives in a static device array of
+ * smcrt_static_scratch_bytes() bytes inside the library, present on every GPU
+ * that loads it until the process exits.  Scenes that need device-resident scene
+ * tables (more than 16 regions or 32 primitives) are refused with
+ * SMCRT_ERR_SCENE.  ADDS the tallies of packets [first, first+count) into
+ * jmean_dev/det_bins_dev on opts->stream (NULL = the default stream).  The first
+ * call on a device looks up the array's device address for that device
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  Every
+ * call shares the one array and clears it at its start: calls that overlap on
+ * the GPU (other streams, other threads) race on it.  If stats is not NULL the
+ * call waits for the kernel (with a host-side limit of the time budget plus
+ * 30 s) and fills it; a run stopped by its time budget then returns
+ * SMCRT_ERR_TIMEOUT.  If stats is NULL the call returns after the launch and such
+ * a stop is NOT reported: pass stats to learn of it. */
 int32_t smcrt_run_device_static(const smcrt_scene* scene, const smcrt_grid* grid,
                                 const smcrt_source* source, const smcrt_detector* dets,
                                 int32_t ndet, const smcrt_options* opts, int64_t first,
@@ -409,6 +430,14 @@ int32_t smcrt_reflect_refract(int32_t precision, const double* I, const double* 
  * else 2 (the bias-test draw is skipped when g == 0)). */
 int32_t smcrt_scatter_dir(int32_t precision, const double* dir_in, const double* g,
                           const double* u, int64_t n, double* dir_out);
+/* Launch state of packets [first, first+npk) of stream `seed` (instance 0): the
+ * emitter of `source` (src/photon.f90: pencil :464-505, point :290-338, uniform
+ * :397-461, circular :214-287, annulus :645-711, focus :340-394) and the launch
+ * layer (src/kernelsMod.f90:275-280, 1-based) as the transport kernels take it.
+ * pos/dir: 3 doubles per packet. */
+int32_t smcrt_emit(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* source,
+                   int32_t precision, int64_t first, int64_t npk, uint64_t seed, double* pos,
+                   double* dir, int32_t* layer);
 /* Philox4x32-10 block for (key, counter): 4 words per request. */
 int32_t smcrt_philox(const uint32_t* key2, const uint32_t* ctr4, int64_t n, uint32_t* out4);
 

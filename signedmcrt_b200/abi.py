@@ -8,7 +8,7 @@ import ctypes as C
 
 import numpy as np
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # status
 OK, ERR_ARG, ERR_SCENE, ERR_CUDA, ERR_DEVICE, ERR_TIMEOUT, ERR_NO_DEVICE = range(7)
@@ -68,7 +68,7 @@ class Options(C.Structure):
                 ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("max_trace_steps", C.c_int32),
                 ("eps", C.c_double), ("normal_h", C.c_double), ("instance", C.c_uint32),
                 ("timeout_ms", C.c_int32), ("stream", C.c_void_p), ("private_stream", C.c_int32),
-                ("tally_copies", C.c_int32)]
+                ("tally_copies", C.c_int32), ("scene_memory", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 class Stats(C.Structure):
@@ -77,10 +77,12 @@ class Stats(C.Structure):
                 ("fresnel_events", C.c_uint64), ("reflections", C.c_uint64),
                 ("kills_step_cap", C.c_uint64), ("kills_error", C.c_uint64), ("rng_draws", C.c_uint64),
                 ("moments", C.c_double * 24), ("kernel_ms", C.c_double), ("device_status", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("reserved", C.c_int32), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
+                ("reserved2", C.c_uint64 * 6)]
 
     def to_dict(self) -> dict:
-        d = {name: getattr(self, name) for name, _ in self._fields_ if name not in ("moments", "reserved")}
+        d = {name: getattr(self, name) for name, _ in self._fields_
+             if name not in ("moments", "reserved", "reserved2")}
         d["moments"] = np.array(self.moments[:], dtype=np.float64)
         return d
 
@@ -180,6 +182,8 @@ SIGNATURES = {
                                C.POINTER(C.c_int32)], C.c_int32),
     "smcrt_scatter_dir": ([C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                            C.c_int64, C.POINTER(C.c_double)], C.c_int32),
+    "smcrt_emit": ([C.POINTER(Scene), C.POINTER(Grid), C.POINTER(Source), C.c_int32, C.c_int64, C.c_int64,
+                    C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32)], C.c_int32),
     "smcrt_philox": ([C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_int64, C.POINTER(C.c_uint32)], C.c_int32),
 }
 

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -34,12 +35,20 @@ int fail(int code, const std::string& msg) {
     } while (0)
 
 // ---------------------------------------------------------------------------
-int validate_scene(const smcrt_scene* s) {
+// param_block: the caller needs the scene inside a launch's parameter block (at
+// most kMaxRegions regions and kMaxPrims primitives: batches, the adjoint, the
+// allocation-free run, the probes and the render); contexts also take larger
+// scenes, up to kMaxRegionsDev / kMaxPrimsDev, kept in device memory.
+int validate_scene(const smcrt_scene* s, bool param_block = true) {
     if (!s || !s->regions || !s->prims) return fail(SMCRT_ERR_ARG, "scene: null pointer");
     if (s->nregions <= 0 || s->nprims <= 0) return fail(SMCRT_ERR_SCENE, "scene: empty");
-    if (s->nregions > kMaxRegions || s->nprims > kMaxPrims)
-        return fail(SMCRT_ERR_SCENE, "scene: at most " + std::to_string(kMaxRegions) + " regions and " +
-                                         std::to_string(kMaxPrims) + " primitives");
+    const int maxr = param_block ? kMaxRegions : kMaxRegionsDev, maxp = param_block ? kMaxPrims : kMaxPrimsDev;
+    if (s->nregions > maxr || s->nprims > maxp)
+        return fail(SMCRT_ERR_SCENE, "scene: at most " + std::to_string(maxr) + " regions and " +
+                                         std::to_string(maxp) + " primitives" +
+                                         (param_block ? std::string(" here (larger scenes run through smcrt_create "
+                                                                    "contexts)")
+                                                      : std::string()));
     for (int i = 0; i < s->nprims; ++i) {
         const smcrt_prim& pr = s->prims[i];
         if (pr.kind < SMCRT_SPHERE || pr.kind > SMCRT_PLANE)
@@ -246,6 +255,8 @@ struct smcrt_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int block = 256, grid_blocks = 0;
     int timeout_ms = 600000;
+    bool big = false;                         // scene tables in device memory (d_scene)
+    void* d_scene = nullptr;
 };
 
 namespace {
@@ -422,6 +433,13 @@ int wait_bounded(smcrt_ctx* c) {
     }
 }
 
+// Bytes of one launch's kernel parameter block (the scene and run settings
+// travel as kernel parameters) and of the counter read-back.
+size_t param_bytes(const smcrt_ctx* c) {
+    return c->precision == SMCRT_FP64 ? sizeof(Params<double>) : sizeof(Params<float>);
+}
+constexpr size_t kCounterBytes = sizeof(unsigned long long) * (1 + C_NUM) + sizeof(double) * 25 + sizeof(int);
+
 int read_stats(smcrt_ctx* c, smcrt_stats* st) {
     unsigned long long cnt[1 + C_NUM];
     double mom[25];
@@ -448,11 +466,61 @@ int read_stats(smcrt_ctx* c, smcrt_stats* st) {
         st->nscatt = mom[24];
         st->kernel_ms = ms;
         st->device_status = status;
+        st->h2d_bytes = param_bytes(c);
+        st->d2h_bytes = kCounterBytes;
     }
     if (status & STATUS_ABORTED)
         return fail(SMCRT_ERR_TIMEOUT, "transport kernel reached its time limit and stopped early");
     if (status & (STATUS_STREAM_EXHAUSTED | STATUS_BAD_INDEX))
         return fail(SMCRT_ERR_DEVICE, "device status flag " + std::to_string(status));
+    return SMCRT_OK;
+}
+
+// Uploads a scene too large for the parameter block (or placed in device memory
+// on request): the tables of the transport precision R and the FP64 tables
+// (boundary events), bounding spheres included, in one device allocation owned
+// by the context.
+template <class R>
+int upload_scene(smcrt_ctx* c, const smcrt_scene* scene, const smcrt_grid* grid, SceneG<R>& g, SceneG<double>& g64,
+                 size_t* total) {
+    std::vector<DPrim<R>> pr;
+    std::vector<DRegion<R>> rg;
+    std::vector<R> bd;
+    R margin = 0;
+    scene_tables(scene, grid, pr, rg, bd, &margin);
+    std::vector<DPrim<double>> pr64;
+    std::vector<DRegion<double>> rg64;
+    std::vector<double> bd64;
+    double margin64 = 0;
+    scene_tables(scene, grid, pr64, rg64, bd64, &margin64);
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t o1 = al(sizeof(DPrim<R>) * pr.size()), o2 = o1 + al(sizeof(DRegion<R>) * rg.size()),
+                 o3 = o2 + al(sizeof(R) * bd.size()), o4 = o3 + al(sizeof(DPrim<double>) * pr64.size()),
+                 o5 = o4 + al(sizeof(DRegion<double>) * rg64.size()), o6 = o5 + al(sizeof(double) * bd64.size());
+    std::vector<unsigned char> host(o6, 0);
+    std::memcpy(host.data(), pr.data(), sizeof(DPrim<R>) * pr.size());
+    std::memcpy(host.data() + o1, rg.data(), sizeof(DRegion<R>) * rg.size());
+    std::memcpy(host.data() + o2, bd.data(), sizeof(R) * bd.size());
+    std::memcpy(host.data() + o3, pr64.data(), sizeof(DPrim<double>) * pr64.size());
+    std::memcpy(host.data() + o4, rg64.data(), sizeof(DRegion<double>) * rg64.size());
+    std::memcpy(host.data() + o5, bd64.data(), sizeof(double) * bd64.size());
+    CK(cudaMalloc(&c->d_scene, o6));
+    CK(cudaMemcpy(c->d_scene, host.data(), o6, cudaMemcpyHostToDevice));
+    unsigned char* d = (unsigned char*)c->d_scene;
+    int has_mods = 0;
+    for (int i = 0; i < scene->nprims; ++i) has_mods |= scene->prims[i].nmods > 0;
+    g.nregions = g64.nregions = scene->nregions;
+    g.nprims = g64.nprims = scene->nprims;
+    g.has_mods = g64.has_mods = has_mods;
+    g.prim = (const DPrim<R>*)d;
+    g.region = (const DRegion<R>*)(d + o1);
+    g.bound = (const R*)(d + o2);
+    g.cull_margin = margin;
+    g64.prim = (const DPrim<double>*)(d + o3);
+    g64.region = (const DRegion<double>*)(d + o4);
+    g64.bound = (const double*)(d + o5);
+    g64.cull_margin = margin64;
+    *total = o6;
     return SMCRT_OK;
 }
 
@@ -490,7 +558,7 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
     g_err.clear();
     if (!out) return fail(SMCRT_ERR_ARG, "out is null");
     *out = nullptr;
-    int rc = validate_scene(scene);
+    int rc = validate_scene(scene, false);
     if (rc) return rc;
     rc = validate_optics(scene);
     if (rc) return rc;
@@ -503,6 +571,9 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
         return fail(SMCRT_ERR_ARG, "source: unknown kind");
     if (ndet < 0 || ndet > kMaxDetectors || (ndet > 0 && !dets))
         return fail(SMCRT_ERR_ARG, "detectors: 0.." + std::to_string(kMaxDetectors) + " supported");
+    if (opts && (opts->scene_memory < 0 || opts->scene_memory > 1))
+        return fail(SMCRT_ERR_ARG, "options: scene_memory must be 0 or 1");
+    const bool big = scene->nregions > kMaxRegions || scene->nprims > kMaxPrims || (opts && opts->scene_memory == 1);
     const int prec = opts ? opts->precision : SMCRT_FP32;
     const int kern = opts ? opts->kernel : SMCRT_KERNEL_PATHLENGTH;
     if (prec != SMCRT_FP32 && prec != SMCRT_FP64) return fail(SMCRT_ERR_ARG, "options: unknown precision");
@@ -561,6 +632,14 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
     CKC(cudaMalloc(&c->d_status, sizeof(int)));
     CKC(cudaEventCreate(&c->ev0));
     CKC(cudaEventCreate(&c->ev1));
+    if (big) {
+        // the scene in device memory: transport-precision tables, then FP64 tables
+        c->big = true;
+        size_t bytes = 0;
+        if (prec == SMCRT_FP64) rc = upload_scene<double>(c, scene, grid, c->pd->gsc, c->pd->gsc64, &bytes);
+        else rc = upload_scene<float>(c, scene, grid, c->pf->gsc, c->pf->gsc64, &bytes);
+        if (rc) return bail(rc);
+    }
 #undef CKC
     rc = occupancy_grid(c, prec, kern, opts ? opts->blocks_per_sm : 0);
     if (rc) return bail(rc);
@@ -580,6 +659,7 @@ void smcrt_destroy(smcrt_ctx* c) {
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    if (c->d_scene) cudaFree(c->d_scene);
     delete c->pf;
     delete c->pd;
     delete c;
@@ -610,6 +690,10 @@ int32_t smcrt_adjoint(smcrt_ctx* c, int64_t nphotons, uint64_t seed, const float
     if (!c || nphotons < 0 || !w_dev || !region_group || !grad) return fail(SMCRT_ERR_ARG, "adjoint: bad arguments");
     if (c->precision != SMCRT_FP32 || c->kernel != SMCRT_KERNEL_PATHLENGTH)
         return fail(SMCRT_ERR_ARG, "adjoint: needs an FP32 pathlength context");
+    if (c->big)
+        return fail(SMCRT_ERR_SCENE, "adjoint: needs a scene of at most " + std::to_string(kMaxRegions) +
+                                         " regions and " + std::to_string(kMaxPrims) + " primitives in the "
+                                         "parameter block");
     if (ngroups < 1 || ngroups > kMaxAdjGroups)
         return fail(SMCRT_ERR_ARG, "adjoint: 1.." + std::to_string(kMaxAdjGroups) + " parameter groups");
     Params<float>& P = *c->pf;
@@ -736,7 +820,11 @@ int32_t smcrt_run(smcrt_ctx* c, int64_t nphotons, uint64_t seed, double* jmean, 
     if (det_bins && c->nbins > 0)
         CK(cudaMemcpyAsync(det_bins, c->d_bins, sizeof(double) * c->nbins, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    return read_stats(c, stats);
+    rc = read_stats(c, stats);
+    if (stats)
+        stats->d2h_bytes += (jmean ? sizeof(double) * (size_t)c->ncell : 0) +
+                            (det_bins && c->nbins > 0 ? sizeof(double) * (size_t)c->nbins : 0);
+    return rc;
 }
 
 int32_t smcrt_replay(smcrt_ctx* c, const double* uniforms, const int64_t* offsets, int64_t npackets, double* jmean,
@@ -762,7 +850,14 @@ int32_t smcrt_replay(smcrt_ctx* c, const double* uniforms, const int64_t* offset
     if (jmean) CK(cudaMemcpy(jmean, c->d_jmean, sizeof(double) * c->ncell, cudaMemcpyDeviceToHost));
     if (det_bins && c->nbins > 0) CK(cudaMemcpy(det_bins, c->d_bins, sizeof(double) * c->nbins, cudaMemcpyDeviceToHost));
     if (states) CK(cudaMemcpy(states, dst.p, sizeof(smcrt_packet_state) * npackets, cudaMemcpyDeviceToHost));
-    return read_stats(c, stats);
+    rc = read_stats(c, stats);
+    if (stats) {
+        stats->h2d_bytes += sizeof(double) * nu + sizeof(int64_t) * (npackets + 1);
+        stats->d2h_bytes += (jmean ? sizeof(double) * (size_t)c->ncell : 0) +
+                            (det_bins && c->nbins > 0 ? sizeof(double) * (size_t)c->nbins : 0) +
+                            (states ? sizeof(smcrt_packet_state) * (size_t)npackets : 0);
+    }
+    return rc;
 }
 
 }  // extern "C"
@@ -1199,6 +1294,8 @@ int run_batched_t(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* nphotons
     done = false;
     const Params<R>* P0 = ctx_params<R>(ctxs[0]);
     if (ctxs[0]->kernel == SMCRT_KERNEL_TEST) return SMCRT_OK;
+    for (int i = 0; i < ninst; ++i)
+        if (ctxs[i]->big) return SMCRT_OK;  // batches hold their scene in the parameter block
     for (int i = 1; i < ninst; ++i)
         if (ctxs[i]->precision != ctxs[0]->precision || ctxs[i]->device != ctxs[0]->device ||
             !same_geometry(*P0, *ctx_params<R>(ctxs[i])))
@@ -1267,11 +1364,12 @@ int32_t smcrt_run_batched(smcrt_ctx* const* ctxs, int32_t ninst, const int64_t* 
 }
 
 // ---------------------------------------------------------------------------
-// Allocation-free run.  Some callers cannot allocate device memory at all: code
-// running inside a CUDA stream capture, host applications that own every byte of
-// device memory through their own pool, or processes whose memory is reserved up
-// front for a fixed budget.  smcrt_run_device_static serves them: it creates no
-// context and calls no cudaMalloc/cudaFree.  The transport kernel's scratch (the
+// Allocation-free run.  Some callers cannot allocate device memory at all: host
+// applications that own every byte of device memory through their own pool
+// allocator, or processes whose device memory is reserved up front for a fixed
+// budget, where a library's own cudaMalloc would fail or break the accounting.
+// smcrt_run_device_static serves them: it creates no context and calls no
+// cudaMalloc/cudaFree.  The transport kernel's scratch (the
 // packet-work counter, the event counters, the device status word) lives in the
 // file-scope array below, loaded with the library on every GPU that uses it and
 // held until the process exits.  Every call shares this one array, so calls that
@@ -1364,7 +1462,20 @@ int run_static_t(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_s
                                         : launch_f32_0(P, B, false, blocks, block, s);
     if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (!stats) return SMCRT_OK;
-    CK(cudaStreamSynchronize(s));
+    // wait with a host-side limit: the kernel's own time budget plus a grace period
+    // (a stream query needs no event, so nothing is created)
+    {
+        const double limit = (double)((opts && opts->timeout_ms > 0) ? opts->timeout_ms : 600000) + 30000.0;
+        const auto w0 = std::chrono::steady_clock::now();
+        for (;;) {
+            const cudaError_t q = cudaStreamQuery(s);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) return fail(SMCRT_ERR_CUDA, std::string("kernel: ") + cudaGetErrorString(q));
+            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+            if (ms > limit) return fail(SMCRT_ERR_TIMEOUT, "transport kernel did not finish within its time limit");
+            std::this_thread::sleep_for(std::chrono::microseconds(ms < 10 ? 20 : 500));
+        }
+    }
     unsigned long long cnt[1 + C_NUM];
     double mom[25];
     int status = 0;
@@ -1571,6 +1682,43 @@ int32_t smcrt_scatter_dir(int32_t precision, const double* dir_in, const double*
     UP(dout, nullptr, sizeof(double) * 3 * n);
     CK(probe_scatter(precision, (const double*)dd.p, (const double*)dg.p, (const double*)du.p, n, (double*)dout.p));
     CK(cudaMemcpy(dir_out, dout.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+    return SMCRT_OK;
+}
+
+int32_t smcrt_emit(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_source* source, int32_t precision,
+                   int64_t first, int64_t npk, uint64_t seed, double* pos, double* dir, int32_t* layer) {
+    g_err.clear();
+    int rc = validate_scene(scene);
+    if (rc) return rc;
+    if (!grid || grid->nxg <= 0 || grid->nyg <= 0 || grid->nzg <= 0 || !(grid->xmax > 0) || !(grid->ymax > 0) ||
+        !(grid->zmax > 0))
+        return fail(SMCRT_ERR_ARG, "grid: need positive voxel counts and half sizes");
+    if (!source || source->kind < SMCRT_SRC_POINT || source->kind > SMCRT_SRC_FOCUS)
+        return fail(SMCRT_ERR_ARG, "source: unknown kind");
+    if (precision != SMCRT_FP32 && precision != SMCRT_FP64) return fail(SMCRT_ERR_ARG, "emit: bad precision");
+    if (first < 0 || npk < 0 || !pos || !dir || !layer) return fail(SMCRT_ERR_ARG, "emit: bad arguments");
+    if (npk == 0) return SMCRT_OK;
+    int dev, nsm;
+    rc = pick_device(dev, nsm);
+    if (rc) return rc;
+    DBuf dp, dd, dl;
+    UP(dp, nullptr, sizeof(double) * 3 * npk);
+    UP(dd, nullptr, sizeof(double) * 3 * npk);
+    UP(dl, nullptr, sizeof(int32_t) * npk);
+    if (precision == SMCRT_FP64) {
+        std::unique_ptr<Params<double>> P(new Params<double>);
+        fill_params(P.get(), scene, grid, source, nullptr, 0, nullptr);
+        P->seed = seed;
+        CK(probe_emit<double>(*P, first, npk, (double*)dp.p, (double*)dd.p, (int*)dl.p));
+    } else {
+        std::unique_ptr<Params<float>> P(new Params<float>);
+        fill_params(P.get(), scene, grid, source, nullptr, 0, nullptr);
+        P->seed = seed;
+        CK(probe_emit<float>(*P, first, npk, (double*)dp.p, (double*)dd.p, (int*)dl.p));
+    }
+    CK(cudaMemcpy(pos, dp.p, sizeof(double) * 3 * npk, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dir, dd.p, sizeof(double) * 3 * npk, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(layer, dl.p, sizeof(int32_t) * npk, cudaMemcpyDeviceToHost));
     return SMCRT_OK;
 }
 

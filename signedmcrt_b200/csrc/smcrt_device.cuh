@@ -6,14 +6,20 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "../../include/smcrt.h"
 
 namespace smcrt {
 
+// Scenes up to kMaxRegions regions and kMaxPrims primitives travel in the
+// launch's parameter block (constant bank: warp-broadcast operands); larger
+// scenes, up to kMaxRegionsDev regions, live in device memory (SceneG).
 constexpr int kMaxPrims = 32;
 constexpr int kMaxRegions = 16;
+constexpr int kMaxRegionsDev = 255;
+constexpr int kMaxPrimsDev = 4096;
 constexpr int kMaxDetectors = 16;
 // Detector bins privatized per CTA as 32-bit counts in shared memory (16 KiB);
 // larger bin sets (camera images) add straight into the global FP64 bins.
@@ -75,6 +81,20 @@ struct SceneT {
     int has_mods, pad;  // some primitive carries modifiers
     DPrim<R> prim[kMaxPrims];
     DRegion<R> region[kMaxRegions];
+};
+
+// A scene in device memory (the same tables behind pointers, read through the
+// L1 cache with warp-uniform addresses), with a bounding sphere per region:
+// bound[4 r .. 4 r + 3] = world centre and radius, radius < 0 when the region
+// has none (see sweep_regions).  cull_margin covers the rounding of the test.
+template <class R>
+struct SceneG {
+    int nregions, nprims;
+    int has_mods, pad;
+    const DPrim<R>* prim;
+    const DRegion<R>* region;
+    const R* bound;
+    R cull_margin;
 };
 
 // pos .dot. transform, src/vector_class.f90:292-304
@@ -224,8 +244,9 @@ __device__ __forceinline__ R eval_prim(const DPrim<R>& pr, V3<R> pos) {
 }
 
 // eval_model (src/sdfs/sdf_base.f90:145-160), CSG ops src/sdfs/sdfModifiers.f90:412-475
-template <class R, bool MODS = true>
-__device__ __forceinline__ R eval_region(const SceneT<R>& sc, int r, V3<R> pos) {
+// S: SceneT (parameter block) or SceneG (device memory).
+template <class R, bool MODS = true, class S = SceneT<R>>
+__device__ __forceinline__ R eval_region(const S& sc, int r, V3<R> pos) {
     const DRegion<R>& g = sc.region[r];
     R d = eval_prim<R, MODS>(sc.prim[g.first], pos);
     for (int i = 1; i < g.n; ++i) {
@@ -245,13 +266,13 @@ __device__ __forceinline__ R eval_region(const SceneT<R>& sc, int r, V3<R> pos) 
 }
 
 // calcNormal, src/sdfs/sdf_base.f90:165-189 (always double)
-template <bool MODS = true>
-__device__ __forceinline__ V3<double> calc_normal(const SceneT<double>& sc, int r, V3<double> p, double h) {
+template <bool MODS = true, class S = SceneT<double>>
+__device__ __forceinline__ V3<double> calc_normal(const S& sc, int r, V3<double> p, double h) {
     const V3<double> xyy{1, -1, -1}, yyx{-1, -1, 1}, yxy{-1, 1, -1}, xxx{1, 1, 1};
-    V3<double> n = xyy * eval_region<double, MODS>(sc, r, p + xyy * h) +
-                   yyx * eval_region<double, MODS>(sc, r, p + yyx * h) +
-                   yxy * eval_region<double, MODS>(sc, r, p + yxy * h) +
-                   xxx * eval_region<double, MODS>(sc, r, p + xxx * h);
+    V3<double> n = xyy * eval_region<double, MODS, S>(sc, r, p + xyy * h) +
+                   yyx * eval_region<double, MODS, S>(sc, r, p + yyx * h) +
+                   yxy * eval_region<double, MODS, S>(sc, r, p + yxy * h) +
+                   xxx * eval_region<double, MODS, S>(sc, r, p + xxx * h);
     double t = len3(n);
     return V3<double>{n.x / t, n.y / t, n.z / t};
 }
@@ -502,6 +523,9 @@ template <class R>
 struct Params {
     SceneT<R> sc;
     SceneT<double> sc64;  // boundary events
+    // scenes beyond the parameter block (the BIG kernel instantiation): device tables
+    SceneG<R> gsc;
+    SceneG<double> gsc64;
     GridT<R> grid;
     SourceT<R> src;
     DetT det[kMaxDetectors];

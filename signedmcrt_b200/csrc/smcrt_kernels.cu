@@ -12,17 +12,18 @@
 
 namespace smcrt {
 
-// Dynamic shared memory of a launch: the CTA's packet slots, then the
-// privatized detector bins.  The kernel needs more than the default 48 KiB
-// opt-in limit, set once per kernel.  Scenes whose primitives carry no
+// Dynamic shared memory of a launch: the CTA's packet slots and work-queue
+// rings, then the privatized detector bins.  The kernel needs more than the
+// default 48 KiB, an opt-in that is a property of the function on the CURRENT
+// device, so it is set before every launch (a host-side call of a few
+// microseconds against launches of milliseconds) rather than once per process:
+// a process may launch on several GPUs.  Scenes whose primitives carry no
 // modifiers run the instantiation compiled without the modifier code
-// (MODS = false); replays always run the general one.
-template <bool REPLAY, bool MODS = true>
-static cudaError_t allow_smem() {
-    static const cudaError_t e = cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, REPLAY, false, false, MODS>,
-                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                      (int)(slots_bytes<SMCRT_R>() + sizeof(unsigned) * kMaxSharedBins));
-    return e;
+// (MODS = false); replays always run the general one; scenes held in device
+// memory run the BIG instantiation.
+template <class K>
+static cudaError_t allow_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 cudaError_t SMCRT_CAT(launch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, const Buffers& B, bool replay, int blocks,
@@ -30,11 +31,30 @@ cudaError_t SMCRT_CAT(launch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, cons
     if (block != kBlock) return cudaErrorInvalidConfiguration;
     const size_t smem = slots_bytes<SMCRT_R>() + sizeof(unsigned) * (size_t)P.sbins;
     const bool mods = P.sc.has_mods != 0;
-    cudaError_t e = replay ? allow_smem<true>() : mods ? allow_smem<false>() : allow_smem<false, false>();
-    if (e != cudaSuccess) return e;
-    if (replay) transport_kernel<SMCRT_R, SMCRT_K, true><<<blocks, kBlock, smem, s>>>(P, B);
-    else if (mods) transport_kernel<SMCRT_R, SMCRT_K, false><<<blocks, kBlock, smem, s>>>(P, B);
-    else transport_kernel<SMCRT_R, SMCRT_K, false, false, false, false><<<blocks, kBlock, smem, s>>>(P, B);
+    cudaError_t e;
+    if (P.gsc.prim) {  // a scene in device memory (replays included)
+        if (replay) {
+            auto k = transport_kernel<SMCRT_R, SMCRT_K, true, false, false, true, true>;
+            if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+            k<<<blocks, kBlock, smem, s>>>(P, B);
+        } else {
+            auto k = transport_kernel<SMCRT_R, SMCRT_K, false, false, false, true, true>;
+            if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+            k<<<blocks, kBlock, smem, s>>>(P, B);
+        }
+    } else if (replay) {
+        auto k = transport_kernel<SMCRT_R, SMCRT_K, true>;
+        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+        k<<<blocks, kBlock, smem, s>>>(P, B);
+    } else if (mods) {
+        auto k = transport_kernel<SMCRT_R, SMCRT_K, false>;
+        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+        k<<<blocks, kBlock, smem, s>>>(P, B);
+    } else {
+        auto k = transport_kernel<SMCRT_R, SMCRT_K, false, false, false, false>;
+        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+        k<<<blocks, kBlock, smem, s>>>(P, B);
+    }
     return cudaGetLastError();
 }
 
@@ -46,19 +66,17 @@ cudaError_t SMCRT_CAT(launch_batch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P
     (void)P; (void)B; (void)blocks; (void)s;
     return cudaErrorNotSupported;
 #else
-    static const cudaError_t attr = cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, false, true>,
-                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         (int)slots_bytes<SMCRT_R>());
-    static const cudaError_t attr0 =
-        cudaFuncSetAttribute(transport_kernel<SMCRT_R, SMCRT_K, false, true, false, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slots_bytes<SMCRT_R>());
-    if (attr != cudaSuccess) return attr;
-    if (attr0 != cudaSuccess) return attr0;
-    if (P.sc.has_mods)
-        transport_kernel<SMCRT_R, SMCRT_K, false, true><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
-    else
-        transport_kernel<SMCRT_R, SMCRT_K, false, true, false, false>
-            <<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
+    const size_t smem = slots_bytes<SMCRT_R>();
+    cudaError_t e;
+    if (P.sc.has_mods) {
+        auto k = transport_kernel<SMCRT_R, SMCRT_K, false, true>;
+        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+        k<<<blocks, kBlock, smem, s>>>(P, B);
+    } else {
+        auto k = transport_kernel<SMCRT_R, SMCRT_K, false, true, false, false>;
+        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+        k<<<blocks, kBlock, smem, s>>>(P, B);
+    }
     return cudaGetLastError();
 #endif
 }
@@ -71,29 +89,29 @@ cudaError_t SMCRT_CAT(launch_adjoint, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>&
     return cudaErrorNotSupported;
 #else
     if (sizeof(SMCRT_R) != 4) return cudaErrorNotSupported;
-    static const cudaError_t attr = cudaFuncSetAttribute(transport_kernel<SMCRT_R, 0, false, false, true>,
-                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         (int)slots_bytes<SMCRT_R>());
-    static const cudaError_t attr0 =
-        cudaFuncSetAttribute(transport_kernel<SMCRT_R, 0, false, false, true, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slots_bytes<SMCRT_R>());
-    if (attr != cudaSuccess) return attr;
-    if (attr0 != cudaSuccess) return attr0;
     if (blocks == 0) return cudaSuccess;
-    if (P.sc.has_mods)
-        transport_kernel<SMCRT_R, 0, false, false, true><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
-    else
-        transport_kernel<SMCRT_R, 0, false, false, true, false><<<blocks, kBlock, slots_bytes<SMCRT_R>(), s>>>(P, B);
+    const size_t smem = slots_bytes<SMCRT_R, true>();
+    cudaError_t e;
+    if (P.sc.has_mods) {
+        auto k = transport_kernel<SMCRT_R, 0, false, false, true>;
+        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+        k<<<blocks, kBlock, smem, s>>>(P, B);
+    } else {
+        auto k = transport_kernel<SMCRT_R, 0, false, false, true, false>;
+        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+        k<<<blocks, kBlock, smem, s>>>(P, B);
+    }
     return cudaGetLastError();
 #endif
 }
 
 cudaError_t SMCRT_CAT(occupancy, SMCRT_TAG, SMCRT_K)(int block, size_t sbins_bytes, int* per_sm) {
     if (block != kBlock) return cudaErrorInvalidConfiguration;
-    cudaError_t e = allow_smem<false>();
+    auto k = transport_kernel<SMCRT_R, SMCRT_K, false>;
+    const size_t smem = slots_bytes<SMCRT_R>() + sbins_bytes;
+    cudaError_t e = allow_smem(k, smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, transport_kernel<SMCRT_R, SMCRT_K, false>, kBlock,
-                                                         slots_bytes<SMCRT_R>() + sbins_bytes);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, kBlock, smem);
 }
 
 }  // namespace smcrt

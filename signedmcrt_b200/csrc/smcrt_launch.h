@@ -3,6 +3,8 @@
 // from smcrt_kernels.cu with -DSMCRT_R/-DSMCRT_TAG/-DSMCRT_K).
 #pragma once
 
+#include <vector>
+
 #include "smcrt_transport.cuh"
 
 namespace smcrt {
@@ -34,14 +36,22 @@ cudaError_t probe_fresnel(int precision, const double* I, const double* N, const
 cudaError_t probe_scatter(int precision, const double* dir, const double* g, const double* u, long long n,
                           double* out);
 cudaError_t probe_philox(const uint32_t* key, const uint32_t* ctr, long long n, uint32_t* out);
+template <class R>
+cudaError_t probe_emit(const Params<R>& P, long long first, long long n, double* pos, double* dir, int* layer);
 
 // SDF voxel render into a device image of samples[0]*samples[1]*samples[2]
 // floats, Fortran order (smcrt_render.cu).
 cudaError_t launch_render(int precision, const smcrt_scene* scene, const int samples[3], const double extent[3],
                           float* d_img, int nsm, cudaStream_t s);
 
-// Scene conversion shared by the API and the probes.
+// Scene conversion shared by the API and the probes: the parameter-block tables
+// (scenes of at most kMaxRegions regions / kMaxPrims primitives), and the
+// device-memory tables of any scene with a bounding sphere per region and the
+// cull margin.
 template <class R>
 void fill_scene(SceneT<R>& d, const smcrt_scene* s);
+template <class R>
+void scene_tables(const smcrt_scene* s, const smcrt_grid* grid, std::vector<DPrim<R>>& prims,
+                  std::vector<DRegion<R>>& regions, std::vector<R>& bounds, R* margin);
 
 }  // namespace smcrt

@@ -163,22 +163,6 @@ __device__ __forceinline__ void emit(const Params<R>& P, Pk<R>& pk, Rng& rng) {
     }
 }
 
-// Launch layer (src/kernelsMod.f90:275-280): innermost containing region.
-template <class R>
-__device__ __forceinline__ int launch_layer(const SceneT<R>& sc, V3<R> p) {
-    int best = 0;
-    R bestv = (R)INFINITY;
-    for (int i = 0; i < sc.nregions; ++i) {
-        R d = eval_region(sc, i, p);
-        if (d > (R)0) d = (R)(-999.0);
-        if (fabs(d) < bestv) {
-            bestv = fabs(d);
-            best = i;
-        }
-    }
-    return best;
-}
-
 // Detector hit test + bin (record_hit_1D/2D, detector_base.f90:106-162).
 __device__ __forceinline__ long long detector_bin(const DetT& D, const double p[3], const double l[3], double value,
                                                   int layer1) {
@@ -246,18 +230,31 @@ __device__ __forceinline__ double* tally_grid(const Params<R>& P, int inst) {
     return P.jtab[b & P.tmask];
 }
 
+// The scene a kernel instantiation reads: the parameter block's, or (BIG) the
+// device-memory tables of a scene too large for it.
+template <bool BIG, class R>
+__device__ __forceinline__ const auto& scene_of(const Params<R>& P) {
+    if constexpr (BIG) return P.gsc;
+    else return P.sc;
+}
+template <bool BIG, class R>
+__device__ __forceinline__ const auto& scene64_of(const Params<R>& P) {
+    if constexpr (BIG) return P.gsc64;
+    else return P.sc64;
+}
+
 // Region optics: the scene's, or the batch instance's.
-template <class R, bool BATCH>
+template <class R, bool BATCH, bool BIG>
 __device__ __forceinline__ R opt_kappa(const Params<R>& P, int inst, int r) {
-    return BATCH ? P.bopt[inst].kappa[r] : P.sc.region[r].kappa;
+    return BATCH ? P.bopt[inst].kappa[r] : scene_of<BIG>(P).region[r].kappa;
 }
-template <class R, bool BATCH>
+template <class R, bool BATCH, bool BIG>
 __device__ __forceinline__ R opt_nidx(const Params<R>& P, int inst, int r) {
-    return BATCH ? P.bopt[inst].nidx[r] : P.sc.region[r].nidx;
+    return BATCH ? P.bopt[inst].nidx[r] : scene_of<BIG>(P).region[r].nidx;
 }
-template <class R, bool BATCH>
+template <class R, bool BATCH, bool BIG>
 __device__ __forceinline__ double opt_nidx64(const Params<R>& P, int inst, int r) {
-    return BATCH ? P.bopt[inst].nidx64[r] : P.sc64.region[r].nidx;
+    return BATCH ? P.bopt[inst].nidx64[r] : scene64_of<BIG>(P).region[r].nidx;
 }
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -313,12 +310,29 @@ struct SweepOut {
     T mn, mna, d0, dsL, dsN;
     int nl, lay;
 };
-template <class T, bool MODS = true>
-__device__ __forceinline__ SweepOut<T> sweep_regions(const SceneT<T>& sc, V3<T> p, int L) {
+//
+// Device-memory scenes (SceneG) skip regions by their bounding spheres.  A
+// region with a bound (a single primitive whose SDF is the exact Euclidean
+// distance -- sphere, box, capsule, segment, cylinder, torus -- under a rigid
+// transform) is skipped when the point lies farther from the sphere than the
+// smallest |d| found so far plus a rounding margin: its value is then positive
+// and larger than that minimum, so it changes none of the outputs (the signed
+// minimum only matters through its sign, and the region contains no point
+// there).  Regions 0 and L are always evaluated (their values are outputs).
+template <class T, bool MODS = true, class S = SceneT<T>>
+__device__ __forceinline__ SweepOut<T> sweep_regions(const S& sc, V3<T> p, int L) {
     SweepOut<T> o{(T)INFINITY, (T)INFINITY, (T)0, (T)0, (T)0, -1, 0};
     T inner = (T)INFINITY;
     for (int i = 0; i < sc.nregions; ++i) {
-        const T d = eval_region<T, MODS>(sc, i, p);
+        if constexpr (!std::is_same<S, SceneT<T>>::value) {
+            const T br = sc.bound[4 * i + 3];
+            if (br >= (T)0 && i != 0 && i != L && o.mna < (T)INFINITY) {
+                const T dx = p.x - sc.bound[4 * i], dy = p.y - sc.bound[4 * i + 1], dz = p.z - sc.bound[4 * i + 2];
+                const T lim = o.mna + sc.cull_margin + br;
+                if (dx * dx + dy * dy + dz * dz > lim * lim) continue;
+            }
+        }
+        const T d = eval_region<T, MODS, S>(sc, i, p);
         o.mn = fmin(o.mn, d);
         o.mna = fmin(o.mna, fabs(d));
         if (i == 0) o.d0 = d;
@@ -339,13 +353,13 @@ __device__ __forceinline__ SweepOut<T> sweep_regions(const SceneT<T>& sc, V3<T> 
 // Single-region evaluations of the crossing path.  They stay inline: an
 // out-of-line function would receive the parameter block by reference and read
 // it through generic loads instead of the constant bank.
-template <class R, bool MODS>
-__device__ __forceinline__ R eval_region_cold(const SceneT<R>& sc, int r, V3<R> p) {
-    return eval_region<R, MODS>(sc, r, p);
+template <class R, bool MODS, class S>
+__device__ __forceinline__ R eval_region_cold(const S& sc, int r, V3<R> p) {
+    return eval_region<R, MODS, S>(sc, r, p);
 }
-template <bool MODS>
-__device__ __forceinline__ V3<double> calc_normal_cold(const SceneT<double>& sc, int r, V3<double> p, double h) {
-    return calc_normal<MODS>(sc, r, p, h);
+template <bool MODS, class S>
+__device__ __forceinline__ V3<double> calc_normal_cold(const S& sc, int r, V3<double> p, double h) {
+    return calc_normal<MODS, S>(sc, r, p, h);
 }
 
 // Step start in grid coordinates (the position does not move during a walk).
@@ -358,10 +372,10 @@ __device__ __forceinline__ V3<R> grid_origin(const GridT<R>& g, const V3<double>
 // Starts a sphere-tracing step of length f.dsdf (body of the while loop at
 // inttau2.f90:63-83): optical depth bookkeeping, then the voxel-walk setup.
 // Returns A_WALK, or -1 when the step starts outside the grid (no tally).
-template <class R, bool BATCH>
+template <class R, bool BATCH, bool BIG>
 __device__ __forceinline__ int start_step(const Params<R>& P, const Pk<R>& pk, Flight<R>& f, Cnt& c, bool& tflag) {
     ++c.steps;
-    const R kap = opt_kappa<R, BATCH>(P, pk.inst, pk.layer);
+    const R kap = opt_kappa<R, BATCH, BIG>(P, pk.inst, pk.layer);
     const R tsdf = f.dsdf * kap;
     f.last = false;
     if (f.taurun + tsdf <= f.tau) {
@@ -533,9 +547,9 @@ __device__ __forceinline__ void start_flight(Flight<R>& f, Rng& rng) {
 }
 
 // Moves through a step that starts outside the grid (no walk), then continues.
-template <class R, bool BATCH, bool ADJ>
+template <class R, bool BATCH, bool ADJ, bool BIG>
 __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c, float* acc) {
-    int a = start_step<R, BATCH>(P, pk, f, c, pk.tflag);
+    int a = start_step<R, BATCH, BIG>(P, pk, f, c, pk.tflag);
     if (a < 0) {
         if (ADJ) adj_track(P, pk, acc, (float)f.dsdf, 0.0f);  // a step outside the grid
         pk.pos = advance(pk.pos, f.dsdf, pk.dir);
@@ -551,11 +565,14 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
 // SMCRT_WALK_SEGMENTS voxel segments.  A packet can pass through several
 // actions in one pass (retire -> launch -> sweep -> walk, interact -> sweep ->
 // walk, sweep -> cross).  `c` counts this thread's events since its last flush.
-template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ, bool MODS>
+template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ, bool MODS, bool BIG>
 __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers& B, Pk<R>& pk, Flight<R>& f,
                                                Stream<R, REPLAY>& rng, Cnt& c, int& act, unsigned long long* s_cnt,
                                                double* s_mom, unsigned* s_bins, float* acc) {
-    const SceneT<R>& sc = P.sc;
+    const auto& sc = scene_of<BIG>(P);
+    const auto& sc64 = scene64_of<BIG>(P);
+    using S = std::decay_t<decltype(sc)>;
+    using S64 = std::decay_t<decltype(sc64)>;
     const int N = sc.nregions;
     const R eps = P.eps;
     // ---- adjoint: the end of a packet's first pass -- add its detector term to C
@@ -741,11 +758,11 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         SweepOut<R> sw;
         bool precise = false, defer = false;
         if (sizeof(R) == 4 && act == A_PRECISE) {
-            const SweepOut<double> s64 = sweep_regions<double, MODS>(P.sc64, pk.pos, L);
+            const SweepOut<double> s64 = sweep_regions<double, MODS, S64>(sc64, pk.pos, L);
             sw = SweepOut<R>{(R)s64.mn, (R)s64.mna, (R)s64.d0, (R)s64.dsL, (R)s64.dsN, s64.nl, s64.lay};
             precise = true;
         } else {
-            sw = sweep_regions<R, MODS>(sc, cv<R>(pk.pos), L);
+            sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L);
             defer = sizeof(R) == 4 && (sw.mna <= (R)2 * eps || f.mode == S_CROSS);
         }
         if (defer) {
@@ -773,7 +790,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                     pk.tflag = true;
                     act = end_flight(P, pk);
                 } else {
-                    act = step_or_skip<R, BATCH, ADJ>(P, pk, f, c, acc);
+                    act = step_or_skip<R, BATCH, ADJ, BIG>(P, pk, f, c, acc);
                 }
             } else if (mode == S_STEP) {
                 if (mn >= (R)0) {  // outside every region (:92-96)
@@ -784,7 +801,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                     pk.flags |= STATUS_STEP_CAP;
                     act = end_flight(P, pk);
                 } else if (mna > eps) {
-                    act = step_or_skip<R, BATCH, ADJ>(P, pk, f, c, acc);
+                    act = step_or_skip<R, BATCH, ADJ, BIG>(P, pk, f, c, acc);
                 } else if (f.taurun >= f.tau || pk.tflag) {
                     act = end_flight(P, pk);  // (:99-102)
                 } else {
@@ -804,19 +821,19 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 }
                 act = A_CROSS;
                 f.mode = S_TOP;
-                if (opt_nidx<R, BATCH>(P, pk.inst, L) != opt_nidx<R, BATCH>(P, pk.inst, nl)) {
+                if (opt_nidx<R, BATCH, BIG>(P, pk.inst, L) != opt_nidx<R, BATCH, BIG>(P, pk.inst, nl)) {
                     int which = -1;
                     if (dsL < (R)0 && dsN < (R)0) {
                         which = (fabs(dsL) <= fabs(dsN)) ? L : nl;
                     } else {
                         R tL, tN;
                         if (precise) {
-                            tL = (R)eval_region_cold<double, MODS>(P.sc64, L, f.x.oldpos);
-                            tN = (R)eval_region_cold<double, MODS>(P.sc64, nl, f.x.oldpos);
+                            tL = (R)eval_region_cold<double, MODS, S64>(sc64, L, f.x.oldpos);
+                            tN = (R)eval_region_cold<double, MODS, S64>(sc64, nl, f.x.oldpos);
                         } else {
                             const V3<R> of = cv<R>(f.x.oldpos);
-                            tL = eval_region_cold<R, MODS>(sc, L, of);
-                            tN = eval_region_cold<R, MODS>(sc, nl, of);
+                            tL = eval_region_cold<R, MODS, S>(sc, L, of);
+                            tN = eval_region_cold<R, MODS, S>(sc, nl, of);
                         }
                         if (tL < (R)0 && tN < (R)0) {
                             which = (tL >= tN) ? L : nl;
@@ -850,9 +867,9 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             const int L = pk.layer, nl = f.x.nl;
             ++c.fres;
             c.sdf += 4;
-            const V3<double> Nn = calc_normal_cold<MODS>(P.sc64, which, pk.pos, P.normal_h);
+            const V3<double> Nn = calc_normal_cold<MODS, S64>(sc64, which, pk.pos, P.normal_h);
             V3<double> I{(double)pk.dir.x, (double)pk.dir.y, (double)pk.dir.z};
-            const double m1 = opt_nidx64<R, BATCH>(P, pk.inst, L), m2 = opt_nidx64<R, BATCH>(P, pk.inst, nl);
+            const double m1 = opt_nidx64<R, BATCH, BIG>(P, pk.inst, L), m2 = opt_nidx64<R, BATCH, BIG>(P, pk.inst, nl);
             const double Rf = fresnel(I, Nn, m1, m2);
             const double u = (double)rng.next();
             const bool refl = u <= Rf;
@@ -897,43 +914,55 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
 #ifndef SMCRT_SLOTS_PER_THREAD
 #define SMCRT_SLOTS_PER_THREAD 2
 #endif
-// Slots per thread: two for FP32 transport (132 bytes a slot); one for FP64
-// (172 bytes), so that a CTA's slots stay within the 227 KiB of shared memory.
+// Slots per thread: two for FP32 transport (124 bytes a slot); one for FP64
+// (168 bytes), so that a CTA's slots stay within the 227 KiB of shared memory.
 template <class R>
 struct SlotCount {
     static constexpr int per_thread = sizeof(R) == 4 ? SMCRT_SLOTS_PER_THREAD : 1;
     static constexpr int n = kBlock * per_thread;
 };
-// Sort groups of the actions a packet can wait in between rounds, in list
-// order: FP64 near-surface sweep, sweep (or a pending crossing), walk, interact,
-// retire/launch.  Each warp's first chunk is fixed (warp w, chunk w), so the
-// costly FP64 chunks at the head of the list go to different warps; the rest of
-// the list goes to whichever warp finishes first.  A_DONE maps to kGroups (not
-// listed).
-// Nibble `act` of SMCRT_GROUP_ORDER is the group of action `act`.
+// Work queues of the actions a packet can wait in between passes, in the order
+// a warp looks for a full chunk of 32: FP64 near-surface sweep, retire/launch,
+// interact, sweep (or a pending crossing), walk.  The rare actions come first
+// so that they are taken as soon as 32 of them wait, and the common ones hold
+// the rest of the CTA's packets.  A_DONE maps to kGroups (never queued).
+// Nibble `act` of SMCRT_GROUP_ORDER is the queue of action `act`.
 #ifndef SMCRT_GROUP_ORDER
-#define SMCRT_GROUP_ORDER 0x05431214u
+#define SMCRT_GROUP_ORDER 0x05123431u
 #endif
 constexpr int kGroups = 5;
 __device__ __forceinline__ int act_group(int act) { return (int)((SMCRT_GROUP_ORDER >> (4 * act)) & 0xFu); }
+// Ring capacity of one queue: a power of two of at least the slots of a CTA (a
+// slot sits in at most one queue, so no queue ever holds more than that).
+constexpr int kQueueCap = 2048;
+constexpr unsigned short kQueueEmpty = 0xFFFFu;
+static_assert(SlotCount<float>::n <= kQueueCap && SlotCount<double>::n <= kQueueCap, "queue ring too small");
+static_assert(SlotCount<float>::n < kQueueEmpty, "slot index collides with the empty mark");
 
-template <class R, int kSlots = SlotCount<R>::n>
+template <class R, bool ADJ, int kSlots = SlotCount<R>::n>
 struct Slots {
     static constexpr int kRW = sizeof(R) / 4;  // 32-bit words per R
-    static constexpr int kUW = 4 * kRW + 3 > 8 ? 4 * kRW + 3 : 8;  // union words
+    // union words: walk (tx, ty, tz, td, step length, ci, cj, ck) or crossing
+    // (position before the step, which, nl)
+    static constexpr int kUW = 5 * kRW + 3 > 8 ? 5 * kRW + 3 : 8;
+    static constexpr int kA = ADJ ? kSlots : 1;
     double px[kSlots], py[kSlots], pz[kSlots];
     R dx[kSlots], dy[kSlots], dz[kSlots], w[kSlots];
-    R tau[kSlots], taurun[kSlots], dsdf[kSlots];
+    R tau[kSlots], taurun[kSlots];
     uint32_t u[kUW][kSlots];
-    // act | layer << 3 | mode << 7 | last << 9 | tflag << 10 | adjoint pass << 11 |
+    // act | mode << 3 | last << 5 | tflag << 6 | adjoint pass << 7 | layer << 8 |
     // pk.flags << 16 | rng.flags << 24
     uint32_t meta[kSlots];
     int steps[kSlots], nscatt[kSlots];
     uint32_t bl[kSlots];  // bounces (<= 1001) | rng.left << 11 | batch instance << 14
-    uint32_t p0[kSlots], p1[kSlots], block[kSlots], ndraws[kSlots];
+    // Philox block counter (replay builds: the injected uniforms consumed); the
+    // draw count of a Philox stream is 4 words a block less the words left
+    uint32_t p0[kSlots], p1[kSlots], block[kSlots];
     uint32_t b0[kSlots], b1[kSlots], b2[kSlots], b3[kSlots];
-    float ctot[kSlots], cpre[kSlots];  // adjoint launches only
+    float ctot[kA], cpre[kA];  // adjoint launches only
 };
+// Regions addressable by the 8-bit layer field of a slot.
+constexpr int kMaxLayerField = 256;
 
 template <class R, int kSlots>
 __device__ __forceinline__ void put_r(uint32_t (*u)[kSlots], int k, int s, R v) {
@@ -952,15 +981,15 @@ __device__ __forceinline__ R get_r(const uint32_t (*u)[kSlots], int k, int s) {
 }
 
 template <class R, bool REPLAY, bool BATCH, bool ADJ>
-__device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params<R>& P, const Buffers& B, Pk<R>& pk,
-                                         Flight<R>& f, Stream<R, REPLAY>& rng) {
+__device__ __forceinline__ int load_slot(const Slots<R, ADJ>& sl, int s, const Params<R>& P, const Buffers& B,
+                                         Pk<R>& pk, Flight<R>& f, Stream<R, REPLAY>& rng) {
     const uint32_t m = sl.meta[s];
     const int act = (int)(m & 7u);
-    pk.layer = (int)((m >> 3) & 15u);
-    f.mode = (int)((m >> 7) & 3u);
-    f.last = (m >> 9) & 1u;
-    pk.tflag = (m >> 10) & 1u;
-    pk.phase = ADJ ? (int)((m >> 11) & 1u) : 0;
+    f.mode = (int)((m >> 3) & 3u);
+    f.last = (m >> 5) & 1u;
+    pk.tflag = (m >> 6) & 1u;
+    pk.phase = ADJ ? (int)((m >> 7) & 1u) : 0;
+    pk.layer = (int)((m >> 8) & 255u);
     pk.flags = (int)((m >> 16) & 255u);
     rng.flags = (int)(m >> 24);
     pk.inst = 0;
@@ -970,7 +999,6 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     pk.weight = sl.w[s];
     f.tau = sl.tau[s];
     f.taurun = sl.taurun[s];
-    f.dsdf = sl.dsdf[s];
     f.steps = sl.steps[s];
     pk.nscatt = sl.nscatt[s];
     const uint32_t bl = sl.bl[s];
@@ -979,8 +1007,13 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
     pk.inst = BATCH ? (int)(bl >> 14) : 0;
     rng.p0 = sl.p0[s];
     rng.p1 = sl.p1[s];
-    rng.block = sl.block[s];
-    rng.ndraws = (int)sl.ndraws[s];
+    if (REPLAY) {
+        rng.block = 0;
+        rng.ndraws = (int)sl.block[s];
+    } else {
+        rng.block = sl.block[s];
+        rng.ndraws = (int)((4u * rng.block - (unsigned)rng.left) / (unsigned)U01<R>::kWords);
+    }
     rng.b0 = sl.b0[s];
     rng.b1 = sl.b1[s];
     rng.b2 = sl.b2[s];
@@ -997,15 +1030,16 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
         rng.inj = B.uniforms + o0;
         rng.ninj = (int)(o1 - o0);
     }
-    constexpr int W = Slots<R>::kRW;
+    constexpr int W = Slots<R, ADJ>::kRW;
     if (act == A_WALK) {
         f.w.tx = get_r<R>(sl.u, 0, s);
         f.w.ty = get_r<R>(sl.u, W, s);
         f.w.tz = get_r<R>(sl.u, 2 * W, s);
         f.w.td = get_r<R>(sl.u, 3 * W, s);
-        f.w.ci = (int)sl.u[4 * W][s];
-        f.w.cj = (int)sl.u[4 * W + 1][s];
-        f.w.ck = (int)sl.u[4 * W + 2][s];
+        f.dsdf = get_r<R>(sl.u, 4 * W, s);
+        f.w.ci = (int)sl.u[5 * W][s];
+        f.w.cj = (int)sl.u[5 * W + 1][s];
+        f.w.ck = (int)sl.u[5 * W + 2][s];
     } else if ((act == A_SWEEP || act == A_PRECISE) && f.mode == S_CROSS) {
         f.x.oldpos.x = get_r<double>(sl.u, 0, s);
         f.x.oldpos.y = get_r<double>(sl.u, 2, s);
@@ -1017,10 +1051,10 @@ __device__ __forceinline__ int load_slot(const Slots<R>& sl, int s, const Params
 }
 
 template <class R, bool REPLAY, bool BATCH, bool ADJ>
-__device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const Pk<R>& pk, const Flight<R>& f,
+__device__ __forceinline__ void store_slot(Slots<R, ADJ>& sl, int s, int act, const Pk<R>& pk, const Flight<R>& f,
                                            const Stream<R, REPLAY>& rng) {
-    sl.meta[s] = (uint32_t)act | ((uint32_t)pk.layer << 3) | ((uint32_t)f.mode << 7) | ((uint32_t)f.last << 9) |
-                 ((uint32_t)pk.tflag << 10) | ((uint32_t)(ADJ ? pk.phase & 1 : 0) << 11) | ((uint32_t)pk.flags << 16) |
+    sl.meta[s] = (uint32_t)act | ((uint32_t)f.mode << 3) | ((uint32_t)f.last << 5) | ((uint32_t)pk.tflag << 6) |
+                 ((uint32_t)(ADJ ? pk.phase & 1 : 0) << 7) | ((uint32_t)pk.layer << 8) | ((uint32_t)pk.flags << 16) |
                  ((uint32_t)rng.flags << 24);
     if (act == A_DONE) return;
     sl.px[s] = pk.pos.x;
@@ -1032,14 +1066,12 @@ __device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const P
     sl.w[s] = pk.weight;
     sl.tau[s] = f.tau;
     sl.taurun[s] = f.taurun;
-    sl.dsdf[s] = f.dsdf;
     sl.steps[s] = f.steps;
     sl.nscatt[s] = pk.nscatt;
     sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 11) | ((uint32_t)(BATCH ? pk.inst : 0) << 14);
     sl.p0[s] = rng.p0;
     sl.p1[s] = rng.p1;
-    sl.block[s] = rng.block;
-    sl.ndraws[s] = (uint32_t)rng.ndraws;
+    sl.block[s] = REPLAY ? (uint32_t)rng.ndraws : rng.block;
     sl.b0[s] = rng.b0;
     sl.b1[s] = rng.b1;
     sl.b2[s] = rng.b2;
@@ -1048,15 +1080,16 @@ __device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const P
         sl.ctot[s] = pk.ctot;
         sl.cpre[s] = pk.cpre;
     }
-    constexpr int W = Slots<R>::kRW;
+    constexpr int W = Slots<R, ADJ>::kRW;
     if (act == A_WALK) {
         put_r<R>(sl.u, 0, s, f.w.tx);
         put_r<R>(sl.u, W, s, f.w.ty);
         put_r<R>(sl.u, 2 * W, s, f.w.tz);
         put_r<R>(sl.u, 3 * W, s, f.w.td);
-        sl.u[4 * W][s] = (uint32_t)f.w.ci;
-        sl.u[4 * W + 1][s] = (uint32_t)f.w.cj;
-        sl.u[4 * W + 2][s] = (uint32_t)f.w.ck;
+        put_r<R>(sl.u, 4 * W, s, f.dsdf);
+        sl.u[5 * W][s] = (uint32_t)f.w.ci;
+        sl.u[5 * W + 1][s] = (uint32_t)f.w.cj;
+        sl.u[5 * W + 2][s] = (uint32_t)f.w.ck;
     } else if ((act == A_SWEEP || act == A_PRECISE) && f.mode == S_CROSS) {
         put_r<double>(sl.u, 0, s, f.x.oldpos.x);
         put_r<double>(sl.u, 2, s, f.x.oldpos.y);
@@ -1066,51 +1099,89 @@ __device__ __forceinline__ void store_slot(Slots<R>& sl, int s, int act, const P
     }
 }
 
-// Dynamic shared memory of one CTA: the slots, then the privatized detector bins.
-template <class R>
+// Dynamic shared memory of one CTA: the slots, the work-queue rings, then the
+// privatized detector bins.
+constexpr size_t kQueueBytes = sizeof(unsigned short) * kGroups * kQueueCap;
+template <class R, bool ADJ = false>
 __host__ __device__ constexpr size_t slots_bytes() {
-    return (sizeof(Slots<R>) + 15) / 16 * 16;
+    return (sizeof(Slots<R, ADJ>) + 15) / 16 * 16 + kQueueBytes;
 }
+
+__device__ __forceinline__ unsigned vload(const unsigned* p) { return *(const volatile unsigned*)p; }
+__device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
+
+// Spin limits of the scheduler's waits.  A queue entry is written a few
+// instructions after its place is claimed, so its wait is short; the idle wait
+// of a warp that finds every queue empty lasts until other warps push work, and
+// is bounded by the launch's time budget (and by this count when there is none).
+constexpr int kEntrySpinLimit = 1 << 22;
+constexpr unsigned kIdleSpinLimit = 1u << 31;
 
 // The persistent, compacted kernel.  KERNEL: smcrt_kernel_kind.  REPLAY:
 // injected streams.
 //
-// A CTA holds SlotCount<R>::n packets in shared memory.  Each round it counting-sorts
-// its live slots by their next action (warp ballots, stable in slot order), then
-// every thread takes items t, t + kBlock, ... of the sorted list, runs one pass
-// of the packet's state machine and writes the packet back.  A warp therefore
-// works on 32 packets that start the pass with the same action, whatever mix of
-// actions the CTA's packets are in; rare actions (boundary events, retire and
-// launch) are gathered across the CTA instead of stalling 31 idle lanes.
+// A CTA holds SlotCount<R>::n packets in shared-memory slots.  Each slot waits
+// in one of kGroups work queues (rings of slot indices in shared memory), the
+// queue of the action its packet does next.  A warp takes a chunk of up to 32
+// slots from one queue -- the first queue in priority order holding a full
+// chunk, else the fullest -- runs one pass of each packet's state machine, writes
+// the packets back and appends each slot to the queue of its next action.  A warp
+// therefore works on 32 packets that start the pass with the same action, and
+// rare actions (boundary events, retire and launch, the FP64 near-surface
+// sweeps) are gathered across the CTA instead of stalling 31 idle lanes.  The
+// warps run independently: no CTA barrier between passes, so a warp never waits
+// for the slowest chunk of the others.
+//
+// Queue protocol: a producer claims ring positions with an atomic add on the
+// queue's tail and writes each slot index there after the slot's data (a
+// block-scope fence in between); a consumer claims positions with a
+// compare-and-swap on the head, waits for each entry to leave the empty mark,
+// reads it and puts the mark back.  A slot is in at most one queue, so no ring
+// holds more than SlotCount<R>::n <= kQueueCap entries and a position is never
+// reused before its previous entry was consumed.  The kernel ends when every
+// slot has found no packet left to launch (or the time budget ran out).
 // MODS = false compiles every distance evaluation without the modifier code,
-// for scenes whose primitives carry no modifiers.
-template <class R, int KERNEL, bool REPLAY, bool BATCH = false, bool ADJ = false, bool MODS = true>
+// for scenes whose primitives carry no modifiers.  BIG reads the scene from
+// device memory (scenes beyond the parameter block's kMaxRegions/kMaxPrims).
+template <class R, int KERNEL, bool REPLAY, bool BATCH = false, bool ADJ = false, bool MODS = true, bool BIG = false>
 __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
                                                                              const Buffers B) {
-    constexpr int Q = SlotCount<R>::per_thread;
-    constexpr int NW = kBlock / 32;
+    constexpr int NS = SlotCount<R>::n;
     __shared__ unsigned long long s_cnt[C_NUM];
     __shared__ double s_mom[25];
-    __shared__ int s_off[kGroups][Q][NW];
-    __shared__ unsigned short s_list[SlotCount<R>::n];
-    __shared__ int s_stop;
-    __shared__ int s_next;  // next unclaimed 32-item chunk of the round's list
+    __shared__ unsigned s_head[kGroups], s_tail[kGroups];
+    __shared__ int s_done;  // slots with no packet left to launch
+    __shared__ int s_stop;  // the time budget ran out (or a wait gave up)
     extern __shared__ __align__(16) unsigned char s_dyn[];
-    Slots<R>& sl = *reinterpret_cast<Slots<R>*>(s_dyn);
-    unsigned* s_bins = reinterpret_cast<unsigned*>(s_dyn + slots_bytes<R>());
+    Slots<R, ADJ>& sl = *reinterpret_cast<Slots<R, ADJ>*>(s_dyn);
+    auto s_q = reinterpret_cast<unsigned short (*)[kQueueCap]>(s_dyn + slots_bytes<R, ADJ>() - kQueueBytes);
+    unsigned* s_bins = reinterpret_cast<unsigned*>(s_dyn + slots_bytes<R, ADJ>());
     const int t = threadIdx.x;
     const unsigned lane = lane_id();
-    const int warp = t >> 5;
     if (t < C_NUM) s_cnt[t] = 0ull;
     if (t < 25) s_mom[t] = 0.0;
     for (int i = t; i < P.sbins; i += kBlock) s_bins[i] = 0u;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) sl.meta[t + q * kBlock] = (uint32_t)A_NEW;
+    // every slot starts empty (A_NEW) in the launch queue
+    const int gnew = act_group(A_NEW);
+    for (int i = t; i < kGroups * kQueueCap; i += kBlock) {
+        const int g = i / kQueueCap, k = i % kQueueCap;
+        s_q[g][k] = (g == gnew && k < NS) ? (unsigned short)k : kQueueEmpty;
+    }
+    for (int i = t; i < NS; i += kBlock) sl.meta[i] = (uint32_t)A_NEW;
+    if (t < kGroups) {
+        s_head[t] = 0u;
+        s_tail[t] = (t == gnew) ? (unsigned)NS : 0u;
+    }
+    if (t == 0) {
+        s_done = 0;
+        s_stop = 0;
+    }
 
     // adjoint: per-thread gradient accumulators [3][kMaxAdjGroups][kBlock]
     __shared__ float s_acc[ADJ ? 3 * kMaxAdjGroups * kBlock : 1];
     if (ADJ)
         for (int i = t; i < 3 * kMaxAdjGroups * kBlock; i += kBlock) s_acc[i] = 0.0f;
+    __syncthreads();
     Pk<R> pk;
     pk.inst = 0;
     pk.phase = 0;
@@ -1118,92 +1189,99 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     Flight<R> f;
     Stream<R, REPLAY> rng;
     Cnt c = {0, 0, 0, 0, 0, 0};
-    const unsigned long long t0 = P.budget_ns ? global_ns() : 0ull;
+    const unsigned long long t0 = global_ns();
     const unsigned lt = (1u << lane) - 1u;
+    unsigned idle = 0;
     for (;;) {
-        __syncthreads();  // the previous round's slot writes are visible
-        // ---- sort the live slots by action: per-warp counts and ranks
-        int a[Q], rank[Q];
+        // ---- claim a chunk: lane 0 picks the queue and takes up to 32 entries
+        int g = -1, take = 0;
+        unsigned h = 0;
+        if (lane == 0) {
+            for (int tries = 0; tries < 256; ++tries) {
+                int best = -1, bavail = 0;
+                unsigned bh = 0;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            a[q] = act_group((int)(sl.meta[t + q * kBlock] & 7u));
-            rank[q] = 0;
-#pragma unroll
-            for (int g = 0; g < kGroups; ++g) {
-                const unsigned m = __ballot_sync(0xffffffffu, a[q] == g);
-                if (a[q] == g) rank[q] = __popc(m & lt);
-                if (lane == 0) s_off[g][q][warp] = __popc(m);
+                for (int k = 0; k < kGroups; ++k) {
+                    const unsigned hk = vload(&s_head[k]);
+                    const int av = (int)(vload(&s_tail[k]) - hk);
+                    if (av > bavail && bavail < 32) {
+                        best = k;
+                        bavail = av;
+                        bh = hk;
+                    }
+                }
+                if (best < 0) break;  // every queue is empty
+                const int n = bavail < 32 ? bavail : 32;
+                if (atomicCAS(&s_head[best], bh, bh + (unsigned)n) == bh) {
+                    g = best;
+                    h = bh;
+                    take = n;
+                    break;
+                }
             }
         }
-        if (t == 0) {
+        take = __shfl_sync(0xffffffffu, take, 0);
+        if (take == 0) {
+            // nothing queued: finished, stopped, or every live packet is in
+            // another warp's hands for now.  The exit is decided for the whole
+            // warp at once: lanes that left the loop alone would leave the others
+            // waiting in the next full-warp shuffle.
+            if (__any_sync(0xffffffffu, vload(&s_done) >= NS || vload(&s_stop))) break;
+            if (lane == 0 && ((P.budget_ns && global_ns() - t0 > P.budget_ns) || ++idle > kIdleSpinLimit)) {
+                atomicOr(B.status, STATUS_ABORTED);
+                s_stop = 1;
+            }
+            __syncwarp();
+            __nanosleep(200);
+            continue;
+        }
+        g = __shfl_sync(0xffffffffu, g, 0);
+        h = __shfl_sync(0xffffffffu, h, 0);
+        int s = -1, act = A_DONE;
+        if ((int)lane < take) {
+            volatile unsigned short* e = &s_q[g][(h + lane) & (unsigned)(kQueueCap - 1)];
+            unsigned short v = *e;
+            for (int spin = 0; v == kQueueEmpty && spin < kEntrySpinLimit; ++spin) v = *e;
+            if (v == kQueueEmpty) {  // never written: give up on this slot and stop the CTA
+                atomicOr(B.status, STATUS_ABORTED);
+                s_stop = 1;
+            } else {
+                *e = kQueueEmpty;
+                s = (int)v;
+            }
+        }
+        __threadfence_block();  // the slot's data was written before its entry
+        if (s >= 0) {
+            act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
+            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins,
+                                                                     s_acc);
+            store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
+        }
+        __threadfence_block();  // the slot's data before the entry that publishes it
+        // ---- queue every slot for its next action
+        const int grp = s >= 0 ? act_group(act) : kGroups;
+#pragma unroll
+        for (int k = 0; k < kGroups; ++k) {
+            const unsigned m = __ballot_sync(0xffffffffu, grp == k);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                unsigned base = 0;
+                if ((int)lane == leader) base = atomicAdd(&s_tail[k], (unsigned)__popc(m));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (grp == k)
+                    s_q[k][(base + (unsigned)__popc(m & lt)) & (unsigned)(kQueueCap - 1)] = (unsigned short)s;
+            }
+        }
+        const unsigned md = __ballot_sync(0xffffffffu, s >= 0 && act == A_DONE);
+        if (lane == 0) {
+            if (md) atomicAdd(&s_done, __popc(md));
             // device-side time budget: past it, stop and flag ABORTED
-            int stop = 0;
             if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
                 atomicOr(B.status, STATUS_ABORTED);
-                stop = 1;
-            }
-            s_stop = stop;
-            s_next = NW;
-        }
-        __syncthreads();
-        // every warp scans the (group, q, warp) counts itself: each group is
-        // contiguous in the list, in slot order
-        int total;
-        {
-            constexpr int E = kGroups * Q * NW;
-            constexpr int PER = (E + 31) / 32;
-            const int* flat = &s_off[0][0][0];
-            int v[PER], sum = 0;
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                const int e = (int)lane * PER + k;
-                v[k] = e < E ? flat[e] : 0;
-                sum += v[k];
-            }
-            int incl = sum;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, d);
-                if ((int)lane >= d) incl += y;
-            }
-            total = __shfl_sync(0xffffffffu, incl, 31);
-            const int excl = incl - sum;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                // offset of entry (a[q], q, warp): held by lane e / PER as element e % PER
-                const int g = a[q] < kGroups ? a[q] : 0;
-                const int e = (g * Q + q) * NW + warp;
-                const int src = e / PER, k = e % PER;
-                int off = __shfl_sync(0xffffffffu, excl, src);
-#pragma unroll
-                for (int kk = 0; kk < PER; ++kk) {
-                    const int vk = __shfl_sync(0xffffffffu, v[kk], src);
-                    if (kk < k) off += vk;
-                }
-                if (a[q] < kGroups) s_list[off + rank[q]] = (unsigned short)(t + q * kBlock);
+                s_stop = 1;
             }
         }
-        const int stop = s_stop;
-        __syncthreads();
-        if (total == 0 || stop) break;
-        // ---- one pass per listed packet: warp w takes 32-item chunks w, w + NW, ...
-        // warp w takes chunk w, so the chunks at the head of the list (the FP64
-        // near-surface group) land on different warps; later chunks go to the
-        // warps that finish first
-        const int nchunks = (total + 31) >> 5;
-        for (int chunk = warp; chunk < nchunks;) {
-            const int i = chunk * 32 + (int)lane;
-            if (i < total) {
-                const int s = s_list[i];
-                int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-                transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins,
-                                                                    s_acc);
-                store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
-            }
-            int next = 0;
-            if (lane == 0) next = atomicAdd(&s_next, 1);
-            chunk = __shfl_sync(0xffffffffu, next, 0);
-        }
+        if (__any_sync(0xffffffffu, vload(&s_stop) != 0)) break;
     }
     // events of packets still in flight (time budget) and since the last retire
     atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);

@@ -205,8 +205,31 @@ def benchmark_settings(name: str) -> Settings:
         st.detectors = [DetectorCfg("annulus", position=(0.0, 0.0, top), direction=(0.0, 0.0, 1.0), layer=8,
                                     radius1=0.1 * k, radius2=0.1 * (k + 1), nbins=10, maxval=1.0)
                         for k in range(10)]
+    elif name == "sphere_scene":
+        sphere_scene_settings(st)
     else:
         raise ConfigError(f"unknown benchmark configuration {name}")
+    return st
+
+
+def sphere_scene_settings(st: Settings | None = None, num_spheres: int = 40) -> Settings:
+    """The reference's res/sphere.toml (the input of its runtime-vs-number-of-SDFs
+    harness, tools/run_sphere_scene.py): `num_spheres` random spheres (n 1.37, no
+    scattering) in a 2 cm box, a uniform source over the top face going -z, a 200^3
+    grid, 1e6 packets, iseed 123456789."""
+    st = st if st is not None else Settings()
+    st.output.overwrite = True
+    st.geometry.geom_name = "sphere_scene"
+    st.geometry.num_spheres = int(num_spheres)
+    st.grid.nxg = st.grid.nyg = st.grid.nzg = 200
+    st.grid.xmax = st.grid.ymax = st.grid.zmax = 1.0
+    st.source.name = "uniform"
+    st.source.direction = (0.0, 0.0, -1.0)
+    st.source.point1 = (-1.0, -1.0, 0.9999999)
+    st.source.point2 = (2.0, 0.0, 0.0)
+    st.source.point3 = (0.0, 2.0, 0.0)
+    st.source.nphotons = 1000000
+    st.simulation.iseed = 123456789
     return st
 
 

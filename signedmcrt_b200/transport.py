@@ -36,7 +36,7 @@ class Transport:
     def __init__(self, array, settings: Settings, *, kernel: str = "pathlength", precision: str = "fp32",
                  end_early: bool = False, stream: int | None = None, block_size: int = 0, blocks_per_sm: int = 0,
                  eps: float = 0.0, normal_h: float = 0.0, max_trace_steps: int = 0, timeout_ms: int = 0,
-                 instance: int = 0, tally_copies: int = 0):
+                 instance: int = 0, tally_copies: int = 0, scene_memory: int = 0):
         self.settings = settings
         self.flat = array if isinstance(array, FlatScene) else FlatScene(array)
         self.grid = settings.grid_c()
@@ -54,6 +54,7 @@ class Transport:
         o.instance = instance
         o.timeout_ms = timeout_ms
         o.tally_copies = tally_copies  # 0: library choice; 1: a single fluence grid
+        o.scene_memory = scene_memory  # 1: the scene from device memory even when it fits the parameter block
         # stream=None: a stream private to this context; an int: that cudaStream_t (0 = default)
         o.stream = stream if stream is not None else None
         o.private_stream = int(stream is None)
@@ -341,6 +342,18 @@ def scatter_dir(dirs, g, u, precision: str = "fp32") -> np.ndarray:
     check(lib().smcrt_scatter_dir(PRECISIONS[precision], abi.dptr(dirs), abi.dptr(g), abi.dptr(u), n,
                                   abi.dptr(out)))
     return out
+
+
+def emit(flat: FlatScene, settings: Settings, first: int, npk: int, seed: int, precision: str = "fp32"):
+    """smcrt_emit: launch positions, directions (npk, 3) and 1-based launch layers of
+    packets [first, first + npk) of stream `seed`, as the transport kernel emits them."""
+    grid, src = settings.grid_c(), settings.source_c()
+    pos = np.empty((npk, 3), dtype=np.float64)
+    dirs = np.empty((npk, 3), dtype=np.float64)
+    layer = np.empty(npk, dtype=np.int32)
+    check(lib().smcrt_emit(flat.ptr(), C.byref(grid), C.byref(src), PRECISIONS[precision], int(first), int(npk),
+                           int(seed), abi.dptr(pos), abi.dptr(dirs), abi.i32ptr(layer)))
+    return pos, dirs, layer
 
 
 def philox(key: np.ndarray, ctr: np.ndarray) -> np.ndarray:

@@ -1,0 +1,63 @@
+"""Scenes beyond the launch's parameter block: the reference's own res/sphere.toml
+(setup_sphere_scene, src/setupGeometry.f90:62-106: 40 spheres + the bounding box
+= 41 regions) runs on the device from scene tables in device memory, with the
+sweep's bounding-sphere cull.  FP64 event counters equal the oracle's exactly
+(the cull skips only regions that cannot change the sweep's outputs), FP32
+transport agrees with the reference-semantics oracle in total path length, and a
+small scene gives the same FP64 histories from device memory as from the
+parameter block."""
+import math
+
+import numpy as np
+import pytest
+
+from signedmcrt_b200 import presets as P
+from tests.test_gpu_parity import COUNT_KEYS, fluence_agrees
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("num_spheres", [17, 40, 120])
+def test_sphere_scene_fp64_matches_oracle_exactly(gpu, oracle, num_spheres):
+    st = P.sphere_scene_settings(num_spheres=num_spheres)
+    arr = P.setup_simulation(st)
+    assert len(arr) == num_spheres + 1
+    n = 20000
+    with gpu.Transport(arr, st, precision="fp64") as tr:
+        g = tr.run(n, 31)
+    o = oracle.run(arr, st, nphotons=n, seed=31, policy=oracle.device_policy("fp64", st.grid_c()))
+    diff = {k: (g.stats[k], o.stats[k]) for k in COUNT_KEYS if g.stats[k] != o.stats[k]}
+    assert not diff, diff
+    assert g.stats["fresnel_events"] > n  # the packets do cross the spheres
+    fluence_agrees(g.jmean, o.jmean)
+
+
+def test_sphere_scene_fp32_total_path_matches_reference_semantics(gpu, oracle):
+    st = P.sphere_scene_settings(num_spheres=40)
+    arr = P.setup_simulation(st)
+    n_or, batches, bsz = 200000, 16, 100000
+    o = oracle.run(arr, st, nphotons=n_or, seed=4242, policy=oracle.reference_policy())
+    tot = []
+    with gpu.Transport(arr, st, precision="fp32") as tr:
+        for b in range(batches):
+            tot.append(tr.run(bsz, 500 + b).jmean.sum() / bsz)
+    tot = np.array(tot)
+    ng = batches * bsz
+    se = tot.std(ddof=1) * math.sqrt(bsz) * math.sqrt(1 / ng + 1 / n_or)
+    assert abs(tot.mean() - o.jmean.sum() / n_or) <= 3 * se, (tot.mean(), o.jmean.sum() / n_or, se)
+
+
+@pytest.mark.parametrize("cfg", ["layered_vessels", "sphere_water"])
+def test_device_memory_scene_equals_parameter_block(gpu, cfg):
+    """The same FP64 packets from the parameter-block scene and from device-memory
+    tables with the cull (layered_vessels: 4 cullable capsules): identical events."""
+    st = P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+    n = 20000
+    with gpu.Transport(arr, st, precision="fp64") as a, \
+            gpu.Transport(arr, st, precision="fp64", scene_memory=1) as b:
+        ra, rb = a.run(n, 5), b.run(n, 5)
+    diff = {k: (ra.stats[k], rb.stats[k]) for k in COUNT_KEYS if ra.stats[k] != rb.stats[k]}
+    assert not diff, diff
+    fluence_agrees(rb.jmean, ra.jmean)
+    assert np.array_equal(ra.bins, rb.bins)
