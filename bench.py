@@ -483,13 +483,16 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="sphere_water",
-                    choices=["sphere_water", "box_slab", "layered_vessels", "batch256", "adjoint", "accuracy",
+                    choices=["sphere_water", "box_slab", "layered_vessels", "sphere_scene", "batch256", "adjoint",
+                             "accuracy",
                              "render"])
     ap.add_argument("--fd-batches", type=int, default=8, help="adjoint: batches of the finite-difference check")
     ap.add_argument("--fd-h", type=float, default=1e-3, help="adjoint: relative finite-difference step")
     ap.add_argument("--batch-scale", type=float, default=1.0, help="batch256: packet counts x this factor")
     ap.add_argument("--packets", type=float, default=0, help="packets per GPU per step (default: the config's)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--num-spheres", type=int, default=40,
+                    help="sphere_scene: spheres of the reference's res/sphere.toml scene (regions = this + 1)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -516,6 +519,8 @@ def main() -> None:
                 print(json.dumps(error_table(cfg, int(args.packets) if args.packets else n)), flush=True)
         return
     st = P.benchmark_settings(args.config)
+    if args.config == "sphere_scene":
+        P.sphere_scene_settings(st, num_spheres=args.num_spheres)
     arr = P.setup_simulation(st)
     flat = FlatScene(arr)
     per_gpu = int(args.packets) if args.packets else int(st.source.nphotons)
@@ -523,7 +528,9 @@ def main() -> None:
     workload = {"workload": f"{args.config}: " + {
         "sphere_water": "sphere r=1 cm (mua .05, mus 50, g .85, n 1.45) in a 4 cm water box, top-hat r=0.5 cm",
         "box_slab": "2 cm box (mua .1, mus 10, g .9, n 1.38), pencil beam",
-        "layered_vessels": "3 layers + 4 capsule vessels, pencil beam, 10 annular detectors"}[args.config],
+        "layered_vessels": "3 layers + 4 capsule vessels, pencil beam, 10 annular detectors",
+        "sphere_scene": f"res/sphere.toml: {args.num_spheres} random spheres (n 1.37) in a 2 cm box "
+                        f"({args.num_spheres + 1} regions, scene in device memory when > 16), uniform source"}[args.config],
         "grid": [g.nxg, g.nyg, g.nzg], "tally": "fp64", "packets_per_gpu_per_step": per_gpu}
 
     if args.impl == "reference":

@@ -1225,9 +1225,13 @@ void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, c
                 double mu = 0.0;
                 scatter(pk.dir, rg.hgg, rg.g2, rng, adj ? &mu : nullptr);
                 if (gi >= 0) {  // roulette mus/kappa, then the phase function
+                    // an albedo-1 region (mua < 1e-9, init_mono, opticalProperties.f90:115-119)
+                    // scatters with probability 1 whatever its parameters: no roulette term
                     const double k = mua_of(pk.layer) + mus_of(pk.layer);
-                    S[0][gi] -= 1.0 / k;
-                    S[1][gi] += 1.0 / mus_of(pk.layer) - 1.0 / k;
+                    if (!(mua_of(pk.layer) < 1e-9)) {
+                        S[0][gi] -= 1.0 / k;
+                        S[1][gi] += 1.0 / mus_of(pk.layer) - 1.0 / k;
+                    }
                     const double hg = A.scene->regions[pk.layer].hgg;
                     S[2][gi] += (hg == 0.0) ? 3.0 * mu : hg_score(hg, mu);
                 }

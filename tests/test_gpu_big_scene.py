@@ -28,7 +28,7 @@ def test_sphere_scene_fp64_matches_oracle_exactly(gpu, oracle, num_spheres):
     o = oracle.run(arr, st, nphotons=n, seed=31, policy=oracle.device_policy("fp64", st.grid_c()))
     diff = {k: (g.stats[k], o.stats[k]) for k in COUNT_KEYS if g.stats[k] != o.stats[k]}
     assert not diff, diff
-    assert g.stats["fresnel_events"] > n  # the packets do cross the spheres
+    assert g.stats["fresnel_events"] > 0.2 * n  # many packets do cross the spheres
     fluence_agrees(g.jmean, o.jmean)
 
 

@@ -88,3 +88,36 @@ def test_reference_gradient_matches_crn_finite_differences(oracle):
     informative = fd.std(axis=0) > 0
     assert informative.sum() >= 12
     assert np.all(np.abs(z[informative]) < 3.0), (z, ref.mean(axis=0), fd.mean(axis=0))
+
+
+def _albedo_one(mus):
+    from signedmcrt_b200 import scene as S
+    st = P.benchmark_settings("box_slab")
+    st.grid.nxg = st.grid.nyg = st.grid.nzg = 20
+    st.source.name = "point"
+    st.source.position = (0.0, 0.0, 0.0)
+    arr = [S.sphere(0.5, S.mono(mus, 0.0, 0.0, 1.0), 1), S.box((2.0, 2.0, 2.0), S.mono(0.0, 0.0, 0.0, 1.0), 2)]
+    return st, arr
+
+
+def test_reference_gradient_in_an_albedo_one_region(oracle):
+    """With the albedo held at 1 the loss depends on mu_a and mu_s only through
+    kappa = mu_s + mu_a, so d/d mu_a = d/d mu_s, and both match common-random-number
+    central finite differences in mu_s (mu_a cannot be stepped down from 0)."""
+    mus, rel, B, n = 10.0, 0.02, 8, 20000
+    st, arr = _albedo_one(mus)
+    w = np.ones((20, 20, 20))
+    pol = oracle.device_policy("fp64", st.grid_c())
+    g, fd = [], []
+    for b in range(B):
+        gb, _ = oracle.adjoint(arr, st, nphotons=n, seed=400 + b, w=w, h=None, region_group=[0, -1], ngroups=1,
+                               policy=pol)
+        g.append(gb[:, 0] / n)
+        lp = oracle.run(_albedo_one(mus * (1 + rel))[1], st, nphotons=n, seed=400 + b, policy=pol).jmean.sum() / n
+        lm = oracle.run(_albedo_one(mus * (1 - rel))[1], st, nphotons=n, seed=400 + b, policy=pol).jmean.sum() / n
+        fd.append((lp - lm) / (2 * rel * mus))
+    g, fd = np.array(g), np.array(fd)
+    m, se = g.mean(axis=0), g.std(axis=0, ddof=1) / np.sqrt(B)
+    assert abs(m[0] - m[1]) <= 3 * np.hypot(se[0], se[1]), (m, se)
+    sfd = fd.std(ddof=1) / np.sqrt(B)
+    assert abs(m[1] - fd.mean()) <= 3 * np.hypot(se[1], sfd), (m[1], fd.mean(), se[1], sfd)
