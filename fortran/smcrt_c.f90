@@ -85,8 +85,8 @@ module smcrt_c
         real(c_double)     :: eps, normal_h
         integer(c_int32_t) :: instance, timeout_ms
         type(c_ptr)        :: stream
-        integer(c_int32_t) :: private_stream, tally_copies, scene_memory
-        integer(c_int32_t) :: reserved(7)
+        integer(c_int32_t) :: private_stream, tally_copies, scene_memory, variance
+        integer(c_int32_t) :: reserved(6)
     end type smcrt_options
 
     type, bind(C) :: smcrt_stats
@@ -95,7 +95,7 @@ module smcrt_c
                               reflections, kills_step_cap, kills_error, rng_draws
         real(c_double)     :: moments(24), kernel_ms
         integer(c_int32_t) :: device_status, reserved
-        integer(c_int64_t) :: h2d_bytes, d2h_bytes, reserved2(6)
+        integer(c_int64_t) :: h2d_bytes, d2h_bytes, variance_overflows, reserved2(5)
     end type smcrt_stats
 
     type, bind(C) :: smcrt_packet_state
@@ -178,6 +178,24 @@ module smcrt_c
             integer(c_int64_t), value :: first, count, seed
             type(c_ptr), value        :: jmean_dev, det_bins_dev, stats
         end function smcrt_run_device
+
+        ! second-moment runs of a context created with opts%variance /= 0
+        integer(c_int32_t) function smcrt_run_moments(ctx, nphotons, seed, jmean, jmean2, det_bins, stats) &
+                bind(C, name="smcrt_run_moments")
+            import :: c_int32_t, c_int64_t, c_ptr
+            type(c_ptr), value        :: ctx
+            integer(c_int64_t), value :: nphotons, seed
+            type(c_ptr), value        :: jmean, jmean2, det_bins, stats
+        end function smcrt_run_moments
+
+        integer(c_int32_t) function smcrt_run_device_moments(ctx, first, count, seed, jmean_dev, jmean2_dev, &
+                                                             det_bins_dev, stats) &
+                bind(C, name="smcrt_run_device_moments")
+            import :: c_int32_t, c_int64_t, c_ptr
+            type(c_ptr), value        :: ctx
+            integer(c_int64_t), value :: first, count, seed
+            type(c_ptr), value        :: jmean_dev, jmean2_dev, det_bins_dev, stats
+        end function smcrt_run_device_moments
 
         integer(c_int32_t) function smcrt_replay(ctx, uniforms, offsets, npackets, jmean, det_bins, states, stats) &
                 bind(C, name="smcrt_replay")

@@ -203,7 +203,13 @@ typedef struct smcrt_options {
                               (up to 255 regions and 4096 primitives, with a
                               bounding-sphere cull of the SDF sweep); 1 = device
                               memory always */
-    int32_t reserved[7];   /* zero */
+    int32_t variance;      /* nonzero: the context also keeps, per voxel, the FP64 sum over
+                              packets of each packet's own score squared (the
+                              history-based second moment of jmean; see
+                              smcrt_run_moments).  Needs a scene in the parameter
+                              block; allocates a voxel-score table per packet slot
+                              (4 KiB each, ~0.8 GB for FP32 on 148 SMs) */
+    int32_t reserved[6];   /* zero */
 } smcrt_options;
 
 /* Event counters of one run (definitions identical in the CPU oracle). */
@@ -229,7 +235,10 @@ typedef struct smcrt_stats {
                                     settings) and any uploaded tables */
     uint64_t d2h_bytes;          /* device-to-host bytes the call moved: tallies copied to
                                     host buffers and the event counters */
-    uint64_t reserved2[6];
+    uint64_t variance_overflows; /* second-moment runs: segments squared on their own because the
+                                    packet's voxel-score table was crowded (their cross terms
+                                    with the packet's other scores in that voxel are missing) */
+    uint64_t reserved2[5];
 } smcrt_stats;
 
 /* Per-packet final state (history replay). */
@@ -305,6 +314,19 @@ int32_t smcrt_autotune(smcrt_ctx* ctx, int64_t trial_packets, uint64_t seed, smc
  * NULL; if not NULL the call synchronises to fill it. */
 int32_t smcrt_run_device(smcrt_ctx* ctx, int64_t first, int64_t count, uint64_t seed,
                          double* jmean_dev, double* det_bins_dev, smcrt_stats* stats);
+
+/* smcrt_run / smcrt_run_device of a context created with options.variance: the
+ * same transport, plus the per-voxel second moment jmean2[v] = sum over packets
+ * of (the packet's total path length in voxel v)^2, FP64, the layout of jmean.
+ * With N packets the per-packet variance of voxel v is jmean2/N - (jmean/N)^2 and
+ * the standard error of jmean/N is sqrt(that / N) (no counterpart in the
+ * reference, which keeps no variance).  _moments copies to HOST buffers (each
+ * may be NULL); _device_moments ADDS into DEVICE buffers on the context stream. */
+int32_t smcrt_run_moments(smcrt_ctx* ctx, int64_t nphotons, uint64_t seed, double* jmean,
+                          double* jmean2, double* det_bins, smcrt_stats* stats);
+int32_t smcrt_run_device_moments(smcrt_ctx* ctx, int64_t first, int64_t count, uint64_t seed,
+                                 double* jmean_dev, double* jmean2_dev, double* det_bins_dev,
+                                 smcrt_stats* stats);
 
 /* Replays packets from caller-supplied uniform streams instead of the counter
  * RNG: packet p consumes uniforms[offsets[p] .. offsets[p+1]) in the reference's

@@ -64,7 +64,8 @@ def lib() -> C.CDLL:
         sig = {
             "oracle_run": ([P(abi.Scene), P(abi.Grid), P(abi.Source), P(abi.Detector), C.c_int32, C.c_int32,
                             C.c_int32, P(Policy), C.c_int64, C.c_int64, C.c_uint64, C.c_uint32, P(C.c_double),
-                            P(C.c_int64), P(C.c_double), P(C.c_double), P(abi.Stats), C.c_void_p], C.c_int32),
+                            P(C.c_int64), P(C.c_double), P(C.c_double), P(abi.Stats), C.c_void_p,
+                            P(C.c_double)], C.c_int32),
             "oracle_detector_bins": ([P(abi.Detector), C.c_int32], C.c_int64),
             "oracle_adjoint": ([P(abi.Scene), P(abi.Grid), P(abi.Source), P(abi.Detector), C.c_int32, P(Policy),
                                 C.c_int64, C.c_uint64, P(C.c_double), P(C.c_double), P(C.c_int32), C.c_int32,
@@ -101,6 +102,7 @@ class OracleResult:
     bins: np.ndarray
     stats: dict
     states: np.ndarray | None = None
+    jmean2: np.ndarray | None = None  # per voxel: sum over packets of the packet's score squared
 
     @property
     def nscatt(self) -> float:
@@ -112,7 +114,7 @@ KERNELS = {"pathlength": abi.KERNEL_PATHLENGTH, "weight": abi.KERNEL_WEIGHT, "te
 
 def run(array, st: Settings, *, nphotons: int, seed: int, policy: Policy | None = None, kernel: str = "pathlength",
         end_early: bool = False, first: int = 0, instance: int = 0, uniforms=None, offsets=None,
-        want_jmean: bool = True, want_states: bool = False) -> OracleResult:
+        want_jmean: bool = True, want_states: bool = False, want_moments: bool = False) -> OracleResult:
     flat = array if isinstance(array, FlatScene) else FlatScene(array)
     grid, src = st.grid_c(), st.source_c()
     dets = st.detectors_c()
@@ -124,6 +126,7 @@ def run(array, st: Settings, *, nphotons: int, seed: int, policy: Policy | None 
     bins = np.zeros(max(nb, 1), dtype=np.float64)
     stats = abi.Stats()
     states = np.zeros(max(nphotons, 1), dtype=abi.PACKET_STATE_DTYPE) if want_states else None
+    j2 = np.empty(g.nxg * g.nyg * g.nzg, dtype=np.float64) if want_moments else None
     u = o = None
     if uniforms is not None:
         u = np.ascontiguousarray(uniforms, dtype=np.float64)
@@ -131,11 +134,13 @@ def run(array, st: Settings, *, nphotons: int, seed: int, policy: Policy | None 
     rc = lib().oracle_run(flat.ptr(), C.byref(grid), C.byref(src), darr, len(dets), KERNELS[kernel],
                           int(end_early), C.byref(pol), first, nphotons, seed, instance, abi.dptr(u), abi.i64ptr(o),
                           abi.dptr(jm), abi.dptr(bins), C.byref(stats),
-                          states.ctypes.data_as(C.c_void_p) if states is not None else None)
+                          states.ctypes.data_as(C.c_void_p) if states is not None else None, abi.dptr(j2))
     if rc != 0:
         raise RuntimeError(f"oracle_run failed ({rc})")
-    return OracleResult(jm.reshape((g.nxg, g.nyg, g.nzg), order="F") if jm is not None else None, bins[:nb],
-                        stats.to_dict(), states[:nphotons] if states is not None else None)
+    shape = (g.nxg, g.nyg, g.nzg)
+    return OracleResult(jm.reshape(shape, order="F") if jm is not None else None, bins[:nb],
+                        stats.to_dict(), states[:nphotons] if states is not None else None,
+                        j2.reshape(shape, order="F") if j2 is not None else None)
 
 
 def adjoint(array, st: Settings, *, nphotons: int, seed: int, w, h, region_group, ngroups: int,

@@ -22,6 +22,7 @@
 #include <cstdint>
 #include <cstring>
 #include <limits>
+#include <unordered_map>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -425,8 +426,12 @@ struct Tally {
     float* j32 = nullptr;
     const double* w = nullptr;  // perturbation MC: voxel weights of the loss
     double* csum = nullptr;     // and the packet's weighted path length
+    // second moment: the packet's own score per voxel, squared into j2 when the
+    // packet ends (history-based variance)
+    std::unordered_map<int64_t, double>* packet = nullptr;
     void add(int64_t idx, double v) {
         if (csum) *csum += w[idx] * v;
+        if (packet) (*packet)[idx] += v;
         if (j32) {
             float* a = j32 + idx;
 #pragma omp atomic
@@ -1127,6 +1132,7 @@ struct RunArgs {
     const double* uniforms;
     const int64_t* offsets;
     Tally tally;
+    double* jmean2 = nullptr;  // per-voxel sum over packets of the packet's score squared
     double* bins;
     smcrt_packet_state* states;
     const struct AdjArgs* adj = nullptr;  // perturbation MC gradient (pathlength kernel)
@@ -1157,6 +1163,23 @@ template <class R, class Rng>
 void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, const RunArgs& A, Rng& rng,
                 Counters& c, int64_t pid) {
     Tally t = A.tally;
+    thread_local std::unordered_map<int64_t, double> scores;
+    if (A.jmean2) {
+        scores.clear();
+        t.packet = &scores;
+    }
+    struct Flush {  // at every return: the packet's squared scores
+        const RunArgs& A;
+        std::unordered_map<int64_t, double>& m;
+        ~Flush() {
+            if (!A.jmean2) return;
+            for (const auto& kv : m) {
+                double* a = A.jmean2 + kv.first;
+#pragma omp atomic
+                *a += kv.second * kv.second;
+            }
+        }
+    } flush{A, scores};
     Packet<R> pk{};
     const AdjArgs* adj = (A.kernel == SMCRT_KERNEL_PATHLENGTH) ? A.adj : nullptr;
     double C = 0, S[3][kAdjGroups] = {};
@@ -1412,7 +1435,7 @@ int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt
                    const oracle_policy* pol, int64_t first, int64_t count, uint64_t seed,
                    uint32_t instance, const double* uniforms, const int64_t* offsets,
                    double* jmean, double* det_bins, smcrt_stats* stats,
-                   smcrt_packet_state* states) {
+                   smcrt_packet_state* states, double* jmean2) {
     if (validate_scene(scene) || !grid || !src || !pol || count < 0 || (ndet > 0 && !dets)) return SMCRT_ERR_ARG;
     if (grid->nxg <= 0 || grid->nyg <= 0 || grid->nzg <= 0) return SMCRT_ERR_ARG;
     if (uniforms && !offsets) return SMCRT_ERR_ARG;
@@ -1461,6 +1484,10 @@ int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt
         A.bins = binbuf.data();
     }
     A.states = states;
+    if (jmean2) {
+        std::fill(jmean2, jmean2 + ncell, 0.0);
+        A.jmean2 = jmean2;
+    }
     int threads = pol->threads > 0 ? pol->threads : oracle_max_threads();
     if (pol->precision == SMCRT_FP32) run_all<float>(A, stats, threads);
     else run_all<double>(A, stats, threads);

@@ -37,8 +37,11 @@ int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt
                    const oracle_policy* pol, int64_t first, int64_t count, uint64_t seed,
                    uint32_t instance, const double* uniforms, const int64_t* offsets,
                    double* jmean, double* det_bins, smcrt_stats* stats,
-                   smcrt_packet_state* states);
+                   smcrt_packet_state* states, double* jmean2);
 
+/* jmean2 (nxg*nyg*nzg or NULL): per voxel, the sum over packets of the square of
+ * the packet's own tally in that voxel (all its segments merged first): the
+ * history-based second moment of the fluence tally. */
 int64_t oracle_detector_bins(const smcrt_detector* dets, int32_t ndet);
 
 /* Perturbation Monte Carlo (likelihood-ratio) reference gradient of

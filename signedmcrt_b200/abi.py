@@ -68,7 +68,8 @@ class Options(C.Structure):
                 ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("max_trace_steps", C.c_int32),
                 ("eps", C.c_double), ("normal_h", C.c_double), ("instance", C.c_uint32),
                 ("timeout_ms", C.c_int32), ("stream", C.c_void_p), ("private_stream", C.c_int32),
-                ("tally_copies", C.c_int32), ("scene_memory", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("tally_copies", C.c_int32), ("scene_memory", C.c_int32), ("variance", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class Stats(C.Structure):
@@ -78,7 +79,7 @@ class Stats(C.Structure):
                 ("kills_step_cap", C.c_uint64), ("kills_error", C.c_uint64), ("rng_draws", C.c_uint64),
                 ("moments", C.c_double * 24), ("kernel_ms", C.c_double), ("device_status", C.c_int32),
                 ("reserved", C.c_int32), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
-                ("reserved2", C.c_uint64 * 6)]
+                ("variance_overflows", C.c_uint64), ("reserved2", C.c_uint64 * 5)]
 
     def to_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_
@@ -146,6 +147,10 @@ SIGNATURES = {
                    C.POINTER(Stats)], C.c_int32),
     "smcrt_run_device": ([C.c_void_p, C.c_int64, C.c_int64, C.c_uint64, C.c_void_p, C.c_void_p,
                           C.POINTER(Stats)], C.c_int32),
+    "smcrt_run_moments": ([C.c_void_p, C.c_int64, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                           C.POINTER(C.c_double), C.POINTER(Stats)], C.c_int32),
+    "smcrt_run_device_moments": ([C.c_void_p, C.c_int64, C.c_int64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(Stats)], C.c_int32),
     "smcrt_replay": ([C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int64, C.POINTER(C.c_double),
                       C.POINTER(C.c_double), C.c_void_p, C.POINTER(Stats)], C.c_int32),
     "smcrt_run_batched": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_uint64),

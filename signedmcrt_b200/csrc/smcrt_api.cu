@@ -257,6 +257,10 @@ struct smcrt_ctx {
     int timeout_ms = 600000;
     bool big = false;                         // scene tables in device memory (d_scene)
     void* d_scene = nullptr;
+    bool variance = false;                    // second-moment runs available
+    uint2* d_vartab = nullptr;                // voxel-score table of every packet slot
+    size_t vartab_bytes = 0;
+    double* d_jmean2 = nullptr;               // second moment of smcrt_run_moments
 };
 
 namespace {
@@ -382,9 +386,12 @@ void set_tally_table(Params<R>* P, double* jm, double* copies, int tc, long long
 }
 
 // Enqueues: reset work/counters/status, then the kernel for [first, first+count).
+// jm2: the second-moment grid of a moments run (nullptr otherwise); its voxel-score
+// tables are emptied first (a run stopped by its time budget leaves entries).
 int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, double* jm, double* bins, bool replay,
-            const double* d_u, const long long* d_off, smcrt_packet_state* d_states) {
+            const double* d_u, const long long* d_off, smcrt_packet_state* d_states, double* jm2 = nullptr) {
     CK(cudaMemsetAsync(c->d_work, 0, sizeof(unsigned long long) * (1 + C_NUM), c->stream));
+    if (jm2) CK(cudaMemsetAsync(c->d_vartab, 0xFF, c->vartab_bytes, c->stream));
     CK(cudaMemsetAsync(c->d_mom, 0, sizeof(double) * 25, c->stream));
     CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
     Buffers B = make_buffers(c, jm, bins);
@@ -402,6 +409,8 @@ int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, doubl
         c->pd->count = count;
         c->pd->seed = seed;
         c->pd->sbins = sb;
+        c->pd->var_tab = jm2 ? c->d_vartab : nullptr;
+        c->pd->jmean2 = jm2;
         set_tally_table(c->pd, jm, c->d_copies, tc, c->ncell);
         rc = launch_f64(c, *c->pd, B, replay, blocks);
     } else {
@@ -409,6 +418,8 @@ int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, doubl
         c->pf->count = count;
         c->pf->seed = seed;
         c->pf->sbins = sb;
+        c->pf->var_tab = jm2 ? c->d_vartab : nullptr;
+        c->pf->jmean2 = jm2;
         set_tally_table(c->pf, jm, c->d_copies, tc, c->ncell);
         rc = launch_f32(c, *c->pf, B, replay, blocks);
     }
@@ -462,6 +473,7 @@ int read_stats(smcrt_ctx* c, smcrt_stats* st) {
         st->kills_step_cap = k[C_STEPCAP];
         st->kills_error = k[C_ERR];
         st->rng_draws = k[C_DRAWS];
+        st->variance_overflows = k[C_VAROVF];
         for (int i = 0; i < 24; ++i) st->moments[i] = mom[i];
         st->nscatt = mom[24];
         st->kernel_ms = ms;
@@ -643,6 +655,20 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
 #undef CKC
     rc = occupancy_grid(c, prec, kern, opts ? opts->blocks_per_sm : 0);
     if (rc) return bail(rc);
+    if (opts && opts->variance) {
+        if (c->big)
+            return bail(fail(SMCRT_ERR_ARG, "options: variance needs a scene in the parameter block (at most " +
+                                                std::to_string(kMaxRegions) + " regions and " +
+                                                std::to_string(kMaxPrims) + " primitives)"));
+        c->variance = true;
+        const size_t slots = (size_t)(prec == SMCRT_FP64 ? SlotCount<double>::n : SlotCount<float>::n);
+        c->vartab_bytes = sizeof(uint2) * (size_t)kVarEntries * slots * (size_t)c->grid_blocks;
+        if (cudaMalloc(&c->d_vartab, c->vartab_bytes) != cudaSuccess)
+            return bail(fail(SMCRT_ERR_CUDA, "variance: cannot allocate " + std::to_string(c->vartab_bytes >> 20) +
+                                                 " MiB of voxel-score tables"));
+        if (cudaMalloc(&c->d_jmean2, sizeof(double) * c->ncell) != cudaSuccess)
+            return bail(fail(SMCRT_ERR_CUDA, "variance: cannot allocate the second-moment grid"));
+    }
     *out = c;
     return SMCRT_OK;
 }
@@ -660,6 +686,8 @@ void smcrt_destroy(smcrt_ctx* c) {
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     if (c->d_scene) cudaFree(c->d_scene);
+    if (c->d_vartab) cudaFree(c->d_vartab);
+    if (c->d_jmean2) cudaFree(c->d_jmean2);
     delete c->pf;
     delete c->pd;
     delete c;
@@ -825,6 +853,54 @@ int32_t smcrt_run(smcrt_ctx* c, int64_t nphotons, uint64_t seed, double* jmean, 
         stats->d2h_bytes += (jmean ? sizeof(double) * (size_t)c->ncell : 0) +
                             (det_bins && c->nbins > 0 ? sizeof(double) * (size_t)c->nbins : 0);
     return rc;
+}
+
+int32_t smcrt_run_moments(smcrt_ctx* c, int64_t nphotons, uint64_t seed, double* jmean, double* jmean2,
+                          double* det_bins, smcrt_stats* stats) {
+    g_err.clear();
+    if (!c) return fail(SMCRT_ERR_ARG, "ctx is null");
+    if (!c->variance) return fail(SMCRT_ERR_ARG, "moments: the context was created without options.variance");
+    if (nphotons < 0) return fail(SMCRT_ERR_ARG, "nphotons < 0");
+    CK(cudaMemsetAsync(c->d_jmean, 0, sizeof(double) * c->ncell, c->stream));
+    CK(cudaMemsetAsync(c->d_jmean2, 0, sizeof(double) * c->ncell, c->stream));
+    CK(cudaMemsetAsync(c->d_bins, 0, sizeof(double) * std::max(1ll, c->nbins), c->stream));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = enqueue(c, 0, nphotons, seed, c->d_jmean, c->d_bins, false, nullptr, nullptr, nullptr, c->d_jmean2);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    rc = wait_bounded(c);
+    if (rc) return rc;
+    if (jmean) CK(cudaMemcpyAsync(jmean, c->d_jmean, sizeof(double) * c->ncell, cudaMemcpyDeviceToHost, c->stream));
+    if (jmean2)
+        CK(cudaMemcpyAsync(jmean2, c->d_jmean2, sizeof(double) * c->ncell, cudaMemcpyDeviceToHost, c->stream));
+    if (det_bins && c->nbins > 0)
+        CK(cudaMemcpyAsync(det_bins, c->d_bins, sizeof(double) * c->nbins, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    rc = read_stats(c, stats);
+    if (stats)
+        stats->d2h_bytes += (jmean ? sizeof(double) * (size_t)c->ncell : 0) +
+                            (jmean2 ? sizeof(double) * (size_t)c->ncell : 0) +
+                            (det_bins && c->nbins > 0 ? sizeof(double) * (size_t)c->nbins : 0);
+    return rc;
+}
+
+int32_t smcrt_run_device_moments(smcrt_ctx* c, int64_t first, int64_t count, uint64_t seed, double* jmean_dev,
+                                 double* jmean2_dev, double* det_bins_dev, smcrt_stats* stats) {
+    g_err.clear();
+    if (!c) return fail(SMCRT_ERR_ARG, "ctx is null");
+    if (!c->variance) return fail(SMCRT_ERR_ARG, "moments: the context was created without options.variance");
+    if (first < 0 || count < 0) return fail(SMCRT_ERR_ARG, "negative packet range");
+    if (!jmean_dev || !jmean2_dev || (c->nbins > 0 && !det_bins_dev))
+        return fail(SMCRT_ERR_ARG, "device buffers are null");
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = enqueue(c, first, count, seed, jmean_dev, det_bins_dev ? det_bins_dev : c->d_bins, false, nullptr,
+                     nullptr, nullptr, jmean2_dev);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    if (!stats) return SMCRT_OK;
+    rc = wait_bounded(c);
+    if (rc) return rc;
+    return read_stats(c, stats);
 }
 
 int32_t smcrt_replay(smcrt_ctx* c, const double* uniforms, const int64_t* offsets, int64_t npackets, double* jmean,

@@ -562,6 +562,11 @@ struct Params {
     double* adj_out;
     int adj_ngroups;
     unsigned char adj_group[kMaxRegions];
+    // second-moment runs (the VAR instantiation): each packet slot's voxel-score
+    // table (kVarEntries (voxel, score) pairs, slot-major over the persistent
+    // grid's CTAs) and the per-voxel sum of squared per-packet scores
+    uint2* var_tab;
+    double* jmean2;
 };
 
 }  // namespace smcrt

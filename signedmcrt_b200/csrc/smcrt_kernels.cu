@@ -32,7 +32,12 @@ cudaError_t SMCRT_CAT(launch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, cons
     const size_t smem = slots_bytes<SMCRT_R>() + sizeof(unsigned) * (size_t)P.sbins;
     const bool mods = P.sc.has_mods != 0;
     cudaError_t e;
-    if (P.gsc.prim) {  // a scene in device memory (replays included)
+    if (P.var_tab) {  // second-moment run: the instantiation with the voxel-score tables
+        if (replay || P.gsc.prim) return cudaErrorNotSupported;
+        auto k = transport_kernel<SMCRT_R, SMCRT_K, false, false, false, true, false, true>;
+        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
+        k<<<blocks, kBlock, smem, s>>>(P, B);
+    } else if (P.gsc.prim) {  // a scene in device memory (replays included)
         if (replay) {
             auto k = transport_kernel<SMCRT_R, SMCRT_K, true, false, false, true, true>;
             if ((e = allow_smem(k, smem)) != cudaSuccess) return e;

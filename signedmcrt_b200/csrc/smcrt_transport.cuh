@@ -31,6 +31,7 @@ enum CounterIdx {
     C_STEPCAP,
     C_ERR,
     C_DRAWS,
+    C_VAROVF,  // second-moment contributions squared alone (score table crowded)
     C_NUM
 };
 
@@ -47,7 +48,7 @@ struct Buffers {
 };
 
 struct Cnt {
-    uint32_t sdf, vox, steps, scat, fres, refl;
+    uint32_t sdf, vox, steps, scat, fres, refl, varovf;
 };
 
 template <class R>
@@ -414,11 +415,61 @@ __device__ __forceinline__ R face_spacing(R v, R dcomp) {
     return v / fabs(dcomp);
 }
 
+// ---------------------------------------------------------------------------
+// History-based second moment of the fluence tally.  The variance of a voxel's
+// tally needs each packet's own total score there (all of its segments in that
+// voxel added first), squared.  Every packet slot owns a table of kVarEntries
+// (voxel, score) pairs in device memory (open addressing, linear probing): a
+// segment adds into its voxel's entry, and the retiring packet adds each entry's
+// squared score to jmean2 and empties the table.  When kVarProbes probes find
+// neither the voxel nor a free entry, that one segment is squared on its own and
+// counted (C_VAROVF): the estimate then lacks the cross terms of that segment.
+constexpr int kVarLog2 = 9;
+constexpr int kVarEntries = 1 << kVarLog2;
+constexpr int kVarProbes = 16;
+constexpr unsigned kVarEmpty = 0xFFFFFFFFu;
+
+__device__ __forceinline__ void var_add(uint2* vt, double* jmean2, int idx, float v, Cnt& c) {
+    unsigned h = ((unsigned)idx * 2654435761u) >> (32 - kVarLog2);
+    for (int k = 0; k < kVarProbes; ++k) {
+        const uint2 e = vt[h];
+        if (e.x == (unsigned)idx) {
+            vt[h].y = __float_as_uint(__uint_as_float(e.y) + v);
+            return;
+        }
+        if (e.x == kVarEmpty) {
+            vt[h] = make_uint2((unsigned)idx, __float_as_uint(v));
+            return;
+        }
+        h = (h + 1u) & (unsigned)(kVarEntries - 1);
+    }
+    atomicAdd(jmean2 + idx, (double)v * (double)v);
+    ++c.varovf;
+}
+
+__device__ __forceinline__ void var_flush(uint2* vt, double* jmean2) {
+    uint4* q = reinterpret_cast<uint4*>(vt);
+    for (int k = 0; k < kVarEntries / 2; ++k) {
+        const uint4 e = q[k];
+        if (e.x == kVarEmpty && e.z == kVarEmpty) continue;
+        if (e.x != kVarEmpty) {
+            const double sc = (double)__uint_as_float(e.y);
+            atomicAdd(jmean2 + e.x, sc * sc);
+        }
+        if (e.z != kVarEmpty) {
+            const double sc = (double)__uint_as_float(e.w);
+            atomicAdd(jmean2 + e.z, sc * sc);
+        }
+        q[k] = make_uint4(kVarEmpty, 0u, kVarEmpty, 0u);
+    }
+}
+
 // One voxel segment of the current step; returns true when the step's walk is over.
 // (ADJ: the adjoint's track terms instead of the fluence tally; on leaving the
 // grid the rest of the step, untallied, still counts for survival.)
-template <class R, bool BATCH, bool ADJ>
-__device__ __forceinline__ bool walk_segment(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c, float* acc) {
+template <class R, bool BATCH, bool ADJ, bool VAR>
+__device__ __forceinline__ bool walk_segment(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c, float* acc,
+                                             uint2* vt) {
     const GridT<R>& g = P.grid;
     const V3<R>& d = pk.dir;
     const R tm = fmin(f.w.tx, fmin(f.w.ty, f.w.tz));
@@ -427,10 +478,12 @@ __device__ __forceinline__ bool walk_segment(const Params<R>& P, Pk<R>& pk, Flig
     if (tm > f.dsdf) {
         if (ADJ) adj_track(P, pk, acc, (float)(f.dsdf - f.w.td), P.adj_w[idx]);
         else atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + idx, (double)(f.dsdf - f.w.td));
+        if (VAR) var_add(vt, P.jmean2, idx, (float)(f.dsdf - f.w.td), c);
         return true;
     }
     if (ADJ) adj_track(P, pk, acc, (float)(tm - f.w.td), P.adj_w[idx]);
     else atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + idx, (double)(tm - f.w.td));
+    if (VAR) var_add(vt, P.jmean2, idx, (float)(tm - f.w.td), c);
     f.w.td = tm;
     bool out = false;
     if (tm == f.w.tx) {
@@ -565,10 +618,10 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
 // SMCRT_WALK_SEGMENTS voxel segments.  A packet can pass through several
 // actions in one pass (retire -> launch -> sweep -> walk, interact -> sweep ->
 // walk, sweep -> cross).  `c` counts this thread's events since its last flush.
-template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ, bool MODS, bool BIG>
+template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ, bool MODS, bool BIG, bool VAR>
 __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers& B, Pk<R>& pk, Flight<R>& f,
                                                Stream<R, REPLAY>& rng, Cnt& c, int& act, unsigned long long* s_cnt,
-                                               double* s_mom, unsigned* s_bins, float* acc) {
+                                               double* s_mom, unsigned* s_bins, float* acc, uint2* vt) {
     const auto& sc = scene_of<BIG>(P);
     const auto& sc64 = scene64_of<BIG>(P);
     using S = std::decay_t<decltype(sc)>;
@@ -589,6 +642,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     }
     // ---- retire a finished packet: detectors (kernelsMod.f90:302-306), counters
     if (act == A_DEATH) {
+        if (VAR) var_flush(vt, P.jmean2);  // the packet's squared voxel scores
         if (!ADJ && P.ndet > 0 && KERNEL != SMCRT_KERNEL_TEST)
             record_detectors(P, BATCH ? B.bins + (long long)pk.inst * P.nbins : B.bins, s_bins, pk.pos.x, pk.pos.y,
                              pk.pos.z, (double)pk.dir.x, (double)pk.dir.y,
@@ -622,7 +676,8 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             atomicAdd(&s_cnt[C_SCAT], (unsigned long long)c.scat);
             atomicAdd(&s_cnt[C_FRES], (unsigned long long)c.fres);
             atomicAdd(&s_cnt[C_REFL], (unsigned long long)c.refl);
-            c = Cnt{0, 0, 0, 0, 0, 0};
+            atomicAdd(&s_cnt[C_VAROVF], (unsigned long long)c.varovf);
+            c = Cnt{0, 0, 0, 0, 0, 0, 0};
         }
         if (REPLAY) {
             smcrt_packet_state& st = B.states[(long long)(((uint64_t)rng.p1 << 32) | rng.p0) - P.first];
@@ -701,8 +756,9 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 pk.tflag = true;
                 act = A_DEATH;
             } else {
-                atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + (ci - 1) + (long long)P.grid.nx * ((cj - 1) + (long long)P.grid.ny * (ck - 1)),
-                          (double)wa);
+                const int cell = (ci - 1) + P.grid.nx * ((cj - 1) + P.grid.ny * (ck - 1));
+                atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + cell, (double)wa);
+                if (VAR) var_add(vt, P.jmean2, cell, (float)wa, c);
                 pk.dir = hg_scatter(pk.dir, hgg, g2, rng);
                 ++c.scat;
                 if (pk.weight < (R)0.01) {  // THRESHOLD, CHANCE (constants.f90:28-30)
@@ -894,7 +950,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // ---- walk voxel segments: at most SMCRT_WALK_SEGMENTS per lane per
     // iteration, so one long walk does not hold up the other lanes' actions
     for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
-        if (walk_segment<R, BATCH, ADJ>(P, pk, f, c, acc)) {
+        if (walk_segment<R, BATCH, ADJ, VAR>(P, pk, f, c, acc, vt)) {
             pk.pos = advance(pk.pos, f.dsdf, pk.dir);
             if (f.last) {
                 act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
@@ -927,17 +983,35 @@ struct SlotCount {
 // so that they are taken as soon as 32 of them wait, and the common ones hold
 // the rest of the CTA's packets.  A_DONE maps to kGroups (never queued).
 // Nibble `act` of SMCRT_GROUP_ORDER is the queue of action `act`.
+#ifndef SMCRT_SCHED
+#define SMCRT_SCHED 2
+#endif
 #ifndef SMCRT_GROUP_ORDER
+#if SMCRT_SCHED == 0
+#define SMCRT_GROUP_ORDER 0x05431214u
+#else
 #define SMCRT_GROUP_ORDER 0x05123431u
+#endif
 #endif
 constexpr int kGroups = 5;
 __device__ __forceinline__ int act_group(int act) { return (int)((SMCRT_GROUP_ORDER >> (4 * act)) & 0xFu); }
 // Ring capacity of one queue: a power of two of at least the slots of a CTA (a
 // slot sits in at most one queue, so no queue ever holds more than that).
 constexpr int kQueueCap = 2048;
+// Bank-aligned queues: per action and bank, a ring of kSubCap slot indices (at
+// least the slots of one bank, SlotCount<R>::n / 32); a chunk is taken when at
+// least kChunkFull lanes find an entry.
+constexpr int kSubCap = 64;
+#ifndef SMCRT_CHUNK_FULL
+#define SMCRT_CHUNK_FULL 24
+#endif
+constexpr int kChunkFull = SMCRT_CHUNK_FULL;
 constexpr unsigned short kQueueEmpty = 0xFFFFu;
 static_assert(SlotCount<float>::n <= kQueueCap && SlotCount<double>::n <= kQueueCap, "queue ring too small");
 static_assert(SlotCount<float>::n < kQueueEmpty, "slot index collides with the empty mark");
+static_assert(SlotCount<float>::n / 32 <= kSubCap && SlotCount<float>::n % 32 == 0 && SlotCount<double>::n % 32 == 0,
+              "bank rings too small");
+static_assert(kGroups * kSubCap * 32 <= kGroups * kQueueCap, "bank rings exceed the queue area");
 
 template <class R, bool ADJ, int kSlots = SlotCount<R>::n>
 struct Slots {
@@ -1143,57 +1217,149 @@ constexpr unsigned kIdleSpinLimit = 1u << 31;
 // MODS = false compiles every distance evaluation without the modifier code,
 // for scenes whose primitives carry no modifiers.  BIG reads the scene from
 // device memory (scenes beyond the parameter block's kMaxRegions/kMaxPrims).
-template <class R, int KERNEL, bool REPLAY, bool BATCH = false, bool ADJ = false, bool MODS = true, bool BIG = false>
+template <class R, int KERNEL, bool REPLAY, bool BATCH = false, bool ADJ = false, bool MODS = true, bool BIG = false,
+          bool VAR = false>
 __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(const __grid_constant__ Params<R> P,
                                                                              const Buffers B) {
     constexpr int NS = SlotCount<R>::n;
     __shared__ unsigned long long s_cnt[C_NUM];
     __shared__ double s_mom[25];
-    __shared__ unsigned s_head[kGroups], s_tail[kGroups];
     __shared__ int s_done;  // slots with no packet left to launch
     __shared__ int s_stop;  // the time budget ran out (or a wait gave up)
     extern __shared__ __align__(16) unsigned char s_dyn[];
     Slots<R, ADJ>& sl = *reinterpret_cast<Slots<R, ADJ>*>(s_dyn);
-    auto s_q = reinterpret_cast<unsigned short (*)[kQueueCap]>(s_dyn + slots_bytes<R, ADJ>() - kQueueBytes);
+    unsigned char* s_qmem = s_dyn + slots_bytes<R, ADJ>() - kQueueBytes;
     unsigned* s_bins = reinterpret_cast<unsigned*>(s_dyn + slots_bytes<R, ADJ>());
     const int t = threadIdx.x;
     const unsigned lane = lane_id();
     if (t < C_NUM) s_cnt[t] = 0ull;
     if (t < 25) s_mom[t] = 0.0;
     for (int i = t; i < P.sbins; i += kBlock) s_bins[i] = 0u;
-    // every slot starts empty (A_NEW) in the launch queue
-    const int gnew = act_group(A_NEW);
-    for (int i = t; i < kGroups * kQueueCap; i += kBlock) {
-        const int g = i / kQueueCap, k = i % kQueueCap;
-        s_q[g][k] = (g == gnew && k < NS) ? (unsigned short)k : kQueueEmpty;
-    }
     for (int i = t; i < NS; i += kBlock) sl.meta[i] = (uint32_t)A_NEW;
-    if (t < kGroups) {
-        s_head[t] = 0u;
-        s_tail[t] = (t == gnew) ? (unsigned)NS : 0u;
-    }
     if (t == 0) {
         s_done = 0;
         s_stop = 0;
     }
-
     // adjoint: per-thread gradient accumulators [3][kMaxAdjGroups][kBlock]
     __shared__ float s_acc[ADJ ? 3 * kMaxAdjGroups * kBlock : 1];
     if (ADJ)
         for (int i = t; i < 3 * kMaxAdjGroups * kBlock; i += kBlock) s_acc[i] = 0.0f;
-    __syncthreads();
     Pk<R> pk;
     pk.inst = 0;
     pk.phase = 0;
     pk.ctot = pk.cpre = 0.0f;
     Flight<R> f;
     Stream<R, REPLAY> rng;
-    Cnt c = {0, 0, 0, 0, 0, 0};
+    Cnt c = {0, 0, 0, 0, 0, 0, 0};
     const unsigned long long t0 = global_ns();
+    // this CTA's voxel-score tables (second-moment runs)
+    uint2* const vbase = VAR ? P.var_tab + (size_t)blockIdx.x * NS * kVarEntries : nullptr;
     const unsigned lt = (1u << lane) - 1u;
+    (void)lt;
+    (void)s_qmem;
+#if SMCRT_SCHED == 0
+    // ---- rounds: each round counting-sorts the live slots by action (warp
+    // ballots and a per-warp scan, stable in slot order) and the warps take
+    // 32-item chunks of the sorted list; three CTA barriers a round
+    constexpr int Q = SlotCount<R>::per_thread;
+    constexpr int NW = kBlock / 32;
+    __shared__ int s_off[kGroups][Q][NW];
+    __shared__ unsigned short s_list[NS];
+    __shared__ int s_next;
+    const int warp = t >> 5;
+    for (;;) {
+        __syncthreads();  // the previous round's slot writes are visible
+        int a[Q], rank[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            a[q] = act_group((int)(sl.meta[t + q * kBlock] & 7u));
+            rank[q] = 0;
+#pragma unroll
+            for (int g = 0; g < kGroups; ++g) {
+                const unsigned m = __ballot_sync(0xffffffffu, a[q] == g);
+                if (a[q] == g) rank[q] = __popc(m & lt);
+                if (lane == 0) s_off[g][q][warp] = __popc(m);
+            }
+        }
+        if (t == 0) {
+            int stop = 0;
+            if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
+                atomicOr(B.status, STATUS_ABORTED);
+                stop = 1;
+            }
+            s_stop = stop;
+            s_next = NW;
+        }
+        __syncthreads();
+        int total;
+        {
+            constexpr int E = kGroups * Q * NW;
+            constexpr int PER = (E + 31) / 32;
+            const int* flat = &s_off[0][0][0];
+            int v[PER], sum = 0;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int e = (int)lane * PER + k;
+                v[k] = e < E ? flat[e] : 0;
+                sum += v[k];
+            }
+            int incl = sum;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, d);
+                if ((int)lane >= d) incl += y;
+            }
+            total = __shfl_sync(0xffffffffu, incl, 31);
+            const int excl = incl - sum;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int g = a[q] < kGroups ? a[q] : 0;
+                const int e = (g * Q + q) * NW + warp;
+                const int src = e / PER, k = e % PER;
+                int off = __shfl_sync(0xffffffffu, excl, src);
+#pragma unroll
+                for (int kk = 0; kk < PER; ++kk) {
+                    const int vk = __shfl_sync(0xffffffffu, v[kk], src);
+                    if (kk < k) off += vk;
+                }
+                if (a[q] < kGroups) s_list[off + rank[q]] = (unsigned short)(t + q * kBlock);
+            }
+        }
+        const int stop = s_stop;
+        __syncthreads();
+        if (total == 0 || stop) break;
+        const int nchunks = (total + 31) >> 5;
+        for (int chunk = warp; chunk < nchunks;) {
+            const int i = chunk * 32 + (int)lane;
+            if (i < total) {
+                const int s = s_list[i];
+                int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
+                transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
+                    P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc,
+                    VAR ? vbase + (size_t)s * kVarEntries : nullptr);
+                store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
+            }
+            int next = 0;
+            if (lane == 0) next = atomicAdd(&s_next, 1);
+            chunk = __shfl_sync(0xffffffffu, next, 0);
+        }
+    }
+#elif SMCRT_SCHED == 1
+    // ---- one ring per action; a warp claims up to 32 consecutive entries
+    __shared__ unsigned s_head[kGroups], s_tail[kGroups];
+    auto s_q = reinterpret_cast<unsigned short (*)[kQueueCap]>(s_qmem);
+    const int gnew = act_group(A_NEW);
+    for (int i = t; i < kGroups * kQueueCap; i += kBlock) {
+        const int g = i / kQueueCap, k = i % kQueueCap;
+        s_q[g][k] = (g == gnew && k < NS) ? (unsigned short)k : kQueueEmpty;
+    }
+    if (t < kGroups) {
+        s_head[t] = 0u;
+        s_tail[t] = (t == gnew) ? (unsigned)NS : 0u;
+    }
+    __syncthreads();
     unsigned idle = 0;
     for (;;) {
-        // ---- claim a chunk: lane 0 picks the queue and takes up to 32 entries
         int g = -1, take = 0;
         unsigned h = 0;
         if (lane == 0) {
@@ -1210,7 +1376,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
                         bh = hk;
                     }
                 }
-                if (best < 0) break;  // every queue is empty
+                if (best < 0) break;
                 const int n = bavail < 32 ? bavail : 32;
                 if (atomicCAS(&s_head[best], bh, bh + (unsigned)n) == bh) {
                     g = best;
@@ -1222,10 +1388,6 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         }
         take = __shfl_sync(0xffffffffu, take, 0);
         if (take == 0) {
-            // nothing queued: finished, stopped, or every live packet is in
-            // another warp's hands for now.  The exit is decided for the whole
-            // warp at once: lanes that left the loop alone would leave the others
-            // waiting in the next full-warp shuffle.
             if (__any_sync(0xffffffffu, vload(&s_done) >= NS || vload(&s_stop))) break;
             if (lane == 0 && ((P.budget_ns && global_ns() - t0 > P.budget_ns) || ++idle > kIdleSpinLimit)) {
                 atomicOr(B.status, STATUS_ABORTED);
@@ -1242,7 +1404,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
             volatile unsigned short* e = &s_q[g][(h + lane) & (unsigned)(kQueueCap - 1)];
             unsigned short v = *e;
             for (int spin = 0; v == kQueueEmpty && spin < kEntrySpinLimit; ++spin) v = *e;
-            if (v == kQueueEmpty) {  // never written: give up on this slot and stop the CTA
+            if (v == kQueueEmpty) {
                 atomicOr(B.status, STATUS_ABORTED);
                 s_stop = 1;
             } else {
@@ -1250,15 +1412,14 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
                 s = (int)v;
             }
         }
-        __threadfence_block();  // the slot's data was written before its entry
+        __threadfence_block();
         if (s >= 0) {
             act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG>(P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins,
-                                                                     s_acc);
+            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
+                P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc, VAR ? vbase + (size_t)s * kVarEntries : nullptr);
             store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
         }
-        __threadfence_block();  // the slot's data before the entry that publishes it
-        // ---- queue every slot for its next action
+        __threadfence_block();
         const int grp = s >= 0 ? act_group(act) : kGroups;
 #pragma unroll
         for (int k = 0; k < kGroups; ++k) {
@@ -1275,7 +1436,6 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         const unsigned md = __ballot_sync(0xffffffffu, s >= 0 && act == A_DONE);
         if (lane == 0) {
             if (md) atomicAdd(&s_done, __popc(md));
-            // device-side time budget: past it, stop and flag ABORTED
             if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
                 atomicOr(B.status, STATUS_ABORTED);
                 s_stop = 1;
@@ -1283,6 +1443,89 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         }
         if (__any_sync(0xffffffffu, vload(&s_stop) != 0)) break;
     }
+#else
+    // ---- bank-aligned queues: slot s always waits in sub-queue (action, s mod 32)
+    // and is always run by lane s mod 32 of some warp, so a chunk's slot loads and
+    // stores hit 32 different shared-memory banks, and a lane pushes its slot
+    // without any warp-wide step.  A warp takes the head entry of its lanes'
+    // sub-queues of one action: the first action (in queue priority order) with
+    // at least kChunkFull lanes' worth waiting, else the one with the most.
+    __shared__ unsigned s_bh[kGroups][32], s_bt[kGroups][32];
+    auto s_q = reinterpret_cast<unsigned short (*)[kSubCap][32]>(s_qmem);  // [group][position][bank]
+    const int gnew = act_group(A_NEW);
+    for (int i = t; i < kGroups * kSubCap * 32; i += kBlock) {
+        const int g = i / (kSubCap * 32), k = (i / 32) % kSubCap, b = i % 32;
+        s_q[g][k][b] = (g == gnew && k < NS / 32) ? (unsigned short)(b + 32 * k) : kQueueEmpty;
+    }
+    if (t < kGroups * 32) {
+        s_bh[t / 32][t % 32] = 0u;
+        s_bt[t / 32][t % 32] = (t / 32 == gnew) ? (unsigned)(NS / 32) : 0u;
+    }
+    __syncthreads();
+    unsigned idle = 0;
+    for (;;) {
+        int g = -1, bestn = 0;
+#pragma unroll
+        for (int k = 0; k < kGroups; ++k) {
+            const bool has = vload(&s_bt[k][lane]) != vload(&s_bh[k][lane]);
+            const int n = __popc(__ballot_sync(0xffffffffu, has));
+            if (n > bestn && bestn < kChunkFull) {
+                g = k;
+                bestn = n;
+            }
+        }
+        if (g < 0) {
+            if (__any_sync(0xffffffffu, vload(&s_done) >= NS || vload(&s_stop))) break;
+            if (lane == 0 && ((P.budget_ns && global_ns() - t0 > P.budget_ns) || ++idle > kIdleSpinLimit)) {
+                atomicOr(B.status, STATUS_ABORTED);
+                s_stop = 1;
+            }
+            __syncwarp();
+            __nanosleep(200);
+            continue;
+        }
+        int s = -1, act = A_DONE;
+        for (int tries = 0; tries < 8; ++tries) {
+            const unsigned h = vload(&s_bh[g][lane]);
+            if (vload(&s_bt[g][lane]) == h) break;  // this lane's sub-queue is empty now
+            if (atomicCAS(&s_bh[g][lane], h, h + 1u) == h) {
+                volatile unsigned short* e = &s_q[g][h & (unsigned)(kSubCap - 1)][lane];
+                unsigned short v = *e;
+                for (int spin = 0; v == kQueueEmpty && spin < kEntrySpinLimit; ++spin) v = *e;
+                if (v == kQueueEmpty) {  // never written: give up on this slot and stop the CTA
+                    atomicOr(B.status, STATUS_ABORTED);
+                    s_stop = 1;
+                } else {
+                    *e = kQueueEmpty;
+                    s = (int)v;
+                }
+                break;
+            }
+        }
+        __threadfence_block();  // the slot's data was written before its entry
+        if (s >= 0) {
+            act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
+            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
+                P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc, VAR ? vbase + (size_t)s * kVarEntries : nullptr);
+            store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
+        }
+        __threadfence_block();  // the slot's data before the entry that publishes it
+        if (s >= 0 && act != A_DONE) {
+            const int k = act_group(act);
+            const unsigned pos = atomicAdd(&s_bt[k][lane], 1u);
+            s_q[k][pos & (unsigned)(kSubCap - 1)][lane] = (unsigned short)s;
+        }
+        const unsigned md = __ballot_sync(0xffffffffu, s >= 0 && act == A_DONE);
+        if (lane == 0) {
+            if (md) atomicAdd(&s_done, __popc(md));
+            if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
+                atomicOr(B.status, STATUS_ABORTED);
+                s_stop = 1;
+            }
+        }
+        if (__any_sync(0xffffffffu, vload(&s_stop) != 0)) break;
+    }
+#endif
     // events of packets still in flight (time budget) and since the last retire
     atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);
     atomicAdd(&s_cnt[C_VOX], (unsigned long long)c.vox);
@@ -1290,6 +1533,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     atomicAdd(&s_cnt[C_SCAT], (unsigned long long)c.scat);
     atomicAdd(&s_cnt[C_FRES], (unsigned long long)c.fres);
     atomicAdd(&s_cnt[C_REFL], (unsigned long long)c.refl);
+    if (VAR) atomicAdd(&s_cnt[C_VAROVF], (unsigned long long)c.varovf);
     __syncthreads();
     if (t < C_NUM && s_cnt[t]) atomicAdd(B.counters + t, s_cnt[t]);
     if (t < 25 && s_mom[t] != 0.0) atomicAdd(B.moments + t, s_mom[t]);

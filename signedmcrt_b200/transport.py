@@ -26,6 +26,7 @@ class RunResult:
     jmean: np.ndarray | None      # (nxg, nyg, nzg) float64, Fortran order
     bins: np.ndarray | None       # concatenated detector bins
     stats: dict
+    jmean2: np.ndarray | None = None  # second moment: sum over packets of each packet's score squared
 
     @property
     def nscatt(self) -> float:
@@ -36,7 +37,7 @@ class Transport:
     def __init__(self, array, settings: Settings, *, kernel: str = "pathlength", precision: str = "fp32",
                  end_early: bool = False, stream: int | None = None, block_size: int = 0, blocks_per_sm: int = 0,
                  eps: float = 0.0, normal_h: float = 0.0, max_trace_steps: int = 0, timeout_ms: int = 0,
-                 instance: int = 0, tally_copies: int = 0, scene_memory: int = 0):
+                 instance: int = 0, tally_copies: int = 0, scene_memory: int = 0, variance: bool = False):
         self.settings = settings
         self.flat = array if isinstance(array, FlatScene) else FlatScene(array)
         self.grid = settings.grid_c()
@@ -55,6 +56,7 @@ class Transport:
         o.timeout_ms = timeout_ms
         o.tally_copies = tally_copies  # 0: library choice; 1: a single fluence grid
         o.scene_memory = scene_memory  # 1: the scene from device memory even when it fits the parameter block
+        o.variance = int(bool(variance))  # keep the per-voxel second moment (run_moments)
         # stream=None: a stream private to this context; an int: that cudaStream_t (0 = default)
         o.stream = stream if stream is not None else None
         o.private_stream = int(stream is None)
@@ -102,6 +104,29 @@ class Transport:
         check(lib().smcrt_run(self._ctx, int(nphotons), int(seed), abi.dptr(jm),
                               abi.dptr(bins) if self.nbins else None, C.byref(st)))
         return RunResult(self._grid_view(jm) if jm is not None else None, bins, st.to_dict())
+
+    def run_moments(self, nphotons: int, seed: int) -> RunResult:
+        """smcrt_run_moments (a context made with variance=True): the run of
+        run(nphotons, seed) plus jmean2, per voxel the sum over packets of the
+        packet's own path length there squared.  The per-packet variance of voxel v
+        is jmean2/N - (jmean/N)^2, the standard error of jmean/N its root over N."""
+        jm = np.empty(self.ncell, dtype=np.float64)
+        j2 = np.empty(self.ncell, dtype=np.float64)
+        bins = np.zeros(max(self.nbins, 0), dtype=np.float64)
+        st = abi.Stats()
+        check(lib().smcrt_run_moments(self._ctx, int(nphotons), int(seed), abi.dptr(jm), abi.dptr(j2),
+                                      abi.dptr(bins) if self.nbins else None, C.byref(st)))
+        return RunResult(self._grid_view(jm), bins, st.to_dict(), self._grid_view(j2))
+
+    def run_device_moments(self, first: int, count: int, seed: int, jmean_dev: int, jmean2_dev: int,
+                           bins_dev: int | None, stats: bool = False) -> dict | None:
+        """smcrt_run_device_moments: adds the tallies and the second moment of packets
+        [first, first+count) into caller-owned device buffers."""
+        st = abi.Stats() if stats else None
+        check(lib().smcrt_run_device_moments(self._ctx, int(first), int(count), int(seed), C.c_void_p(jmean_dev),
+                                             C.c_void_p(jmean2_dev), C.c_void_p(bins_dev) if bins_dev else None,
+                                             C.byref(st) if st is not None else None))
+        return st.to_dict() if st is not None else None
 
     def adjoint(self, nphotons: int, seed: int, w_dev: int, gbins_dev: int | None, region_group,
                 ngroups: int) -> tuple[np.ndarray, dict]:
