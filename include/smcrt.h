@@ -181,9 +181,9 @@ typedef struct smcrt_options {
     int32_t block_size;    /* threads per CTA: 0 or 640 (a CTA holds 1280 FP32 / 640 FP64 packets) */
     int32_t blocks_per_sm; /* 0 = library default (persistent grid = SMs * this) */
     int32_t max_trace_steps; /* per tauint2 sphere-trace step cap; 0 = 1,000,000 */
-    double eps;            /* surface epsilon; <= 0 selects the default policy:
-                              1e-8 (FP64, the reference value, inttau2.f90:44) or
-                              max(1e-8, 8 ulp(largest grid half-size)) in FP32 */
+    double eps;            /* surface epsilon; <= 0 selects the reference's 1e-8
+                              (inttau2.f90:44) in both precisions (FP32 transport
+                              takes every decision against it in FP64) */
     double normal_h;       /* finite-difference step of the normal; <= 0 -> 1e-6
                               (sdf_base.f90:176); normals are evaluated in FP64 */
     uint32_t instance;     /* RNG stream id (second counter word) */

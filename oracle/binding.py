@@ -34,14 +34,10 @@ def reference_policy(threads: int = 0, tally_f32: bool = False) -> Policy:
 
 
 def device_policy(precision: str, grid: abi.Grid, threads: int = 0) -> Policy:
-    """The GPU algorithm: integer voxel walk, FP64 boundary events, default epsilon;
-    in FP32, sweeps within 2 eps of a surface and after crossing steps in FP64."""
-    if precision == "fp64":
-        eps = 1e-8
-    else:
-        L = max(grid.xmax, grid.ymax, grid.zmax)
-        m, e = np.frexp(L)
-        eps = max(1e-8, 8.0 * np.ldexp(1.0, int(e) - 24))
+    """The GPU algorithm: integer voxel walk, FP64 boundary events, the reference's
+    eps; in FP32, sweeps within 16 FP32 ulps of a surface (of the scene size) and
+    after crossing steps in FP64."""
+    eps = 1e-8
     near = 1 if precision == "fp32" else 0
     return Policy(abi.FP32 if precision == "fp32" else abi.FP64, 0, 1, 0, threads, near, eps, 1e-8, 1e-6, 0)
 

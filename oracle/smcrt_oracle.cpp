@@ -470,6 +470,7 @@ struct Pol {
     bool ref_dda, crossing_f64;
     bool kill_le;  // device semantics: d <= eps at the start of a flight counts as on the surface
     bool near_f64; // device FP32 semantics: near-surface and crossing sweeps in FP64 (see sweep)
+    double near_band = 0;  // ... closer than this to a surface
     int64_t max_steps;
 };
 
@@ -555,8 +556,11 @@ bool update_grids_ref(const GridD& g, V3<R> pos, V3<R> dir, R dsdf, R delta, Tal
 // update_grids, but crossings advance the cell index by +-1 and distances are
 // measured from the segment start, so no re-indexing from snapped positions.
 template <class R>
-bool update_grids_int(const GridD& g, V3<R> pos, V3<R> dir, R dsdf, Tally& t, Counters& c, bool& tflag) {
-    V3<R> o{pos.x + (R)g.xmax, pos.y + (R)g.ymax, pos.z + (R)g.zmax};
+// The start cell and the distances to its faces come from the FP64 position (an
+// FP32 coordinate within an ulp of a grid face could round onto it); the walk
+// itself runs in R.
+bool update_grids_int(const GridD& g, V3<double> pos, V3<R> dir, R dsdf, Tally& t, Counters& c, bool& tflag) {
+    const V3<double> o{pos.x + g.xmax, pos.y + g.ymax, pos.z + g.zmax};
     int ci, cj, ck;
     voxel_of(g, o, ci, cj, ck);
     if (ci == -1 || cj == -1 || ck == -1) {
@@ -568,13 +572,15 @@ bool update_grids_int(const GridD& g, V3<R> pos, V3<R> dir, R dsdf, Tally& t, Co
     const int sx = dir.x > 0 ? 1 : (dir.x < 0 ? -1 : 0);
     const int sy = dir.y > 0 ? 1 : (dir.y < 0 ? -1 : 0);
     const int sz = dir.z > 0 ? 1 : (dir.z < 0 ? -1 : 0);
-    auto tnext = [&](int cell, int s, R v, R o1, R d1) -> R {
+    // the first faces at FP64 multiples of the FP64 voxel size
+    auto tnext = [&](int cell, int s, double v, double o1, R d1) -> R {
         if (s == 0) return big;
-        R face = (R)(s > 0 ? cell : cell - 1) * v;
-        R tt = (face - o1) / d1;
+        const double face = (double)(s > 0 ? cell : cell - 1) * v;
+        R tt = (R)(face - o1) / d1;
         return tt < (R)0 ? (R)0 : tt;
     };
-    R tx = tnext(ci, sx, vx, o.x, dir.x), ty = tnext(cj, sy, vy, o.y, dir.y), tz = tnext(ck, sz, vz, o.z, dir.z);
+    const double vxd = 2.0 * g.xmax / g.nx, vyd = 2.0 * g.ymax / g.ny, vzd = 2.0 * g.zmax / g.nz;
+    R tx = tnext(ci, sx, vxd, o.x, dir.x), ty = tnext(cj, sy, vyd, o.y, dir.y), tz = tnext(ck, sz, vzd, o.z, dir.z);
     R d = 0;
     for (;;) {
         R tm = std::min(tx, std::min(ty, tz));
@@ -617,7 +623,8 @@ inline V3<double> advance(V3<double> p, R d, V3<R> dir) {
 // precision R, their signed minimum, minimum |d|, the first region containing the
 // point (-1: none) and the innermost containing region (the launch layer; 0 when
 // none contains it).  Device FP32 semantics (pol.near_f64), as the GPU's FP32
-// kernels do it: a sweep whose FP32 minimum |d| is within 2 eps of a surface, and
+// kernels do it: a sweep whose FP32 minimum |d| is within pol.near_band of a
+// surface (16 FP32 ulps of the scene size, at least 2 eps), and
 // every sweep after a crossing step (force64), is taken instead in FP64 at the
 // FP64 position with the FP64 scene; its values are rounded to R and its region
 // indices come from the FP64 values.
@@ -653,7 +660,7 @@ SweepRes<R> sweep(const Scene<R>& sc, const Scene<double>& sc64, const Pol& pol,
         const V3<R> p = cv<R>(pos);
         for (int i = 0; i < N; ++i) out[i] = eval_region(sc, i, p);
         sweep_stats(out, N, o.mn, o.mna, o.nl, o.lay);
-        if (!pol.near_f64 || sizeof(R) == 8 || o.mna > (R)2 * (R)pol.eps) return o;
+        if (!pol.near_f64 || sizeof(R) == 8 || o.mna > (R)pol.near_band) return o;
     }
     thread_local std::vector<double> v64;
     v64.resize(N);
@@ -731,7 +738,7 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
                 if (len) len[pk.layer] += (double)dsdf;
                 oldpos = pos;
                 ok = pol.ref_dda ? update_grids_ref(g, cv<R>(oldpos), dir, dsdf, (R)pol.delta, t, c, pk.tflag)
-                                 : update_grids_int(g, cv<R>(oldpos), dir, dsdf, t, c, pk.tflag);
+                                 : update_grids_int(g, oldpos, dir, dsdf, t, c, pk.tflag);
                 pos = advance(pos, dsdf, dir);
             } else {
                 dsdf = (tau - taurun) / kap;
@@ -740,7 +747,7 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
                 oldpos = pos;
                 pos = advance(pos, dsdf, dir);
                 ok = pol.ref_dda ? update_grids_ref(g, cv<R>(oldpos), dir, dsdf, (R)pol.delta, t, c, pk.tflag)
-                                 : update_grids_int(g, cv<R>(oldpos), dir, dsdf, t, c, pk.tflag);
+                                 : update_grids_int(g, oldpos, dir, dsdf, t, c, pk.tflag);
                 if (!ok) break;
                 break;
             }
@@ -1119,6 +1126,14 @@ int64_t det_bin(const Det& D, const double p[3], const double l[3], double value
 
 // ---------------------------------------------------------------------------
 // The packet loops (src/kernelsMod.f90).
+// The GPU's FP32 near-surface band: 16 FP32 ulps of the largest grid half-size,
+// at least twice eps.
+inline double near_band(const smcrt_grid* g, double eps) {
+    int e;
+    std::frexp(std::max(g->xmax, std::max(g->ymax, g->zmax)), &e);
+    return std::max(2.0 * eps, 16.0 * std::ldexp(1.0, e - 24));
+}
+
 struct RunArgs {
     const smcrt_scene* scene;
     const smcrt_grid* grid;
@@ -1222,7 +1237,7 @@ void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, c
             R wa = pk.weight * ((R)1 - rg.albedo);
             pk.weight = pk.weight - wa;
             int ci, cj, ck;
-            voxel_of(g, V3<R>{(R)pk.pos.x + (R)g.xmax, (R)pk.pos.y + (R)g.ymax, (R)pk.pos.z + (R)g.zmax}, ci, cj, ck);
+            voxel_of(g, V3<double>{pk.pos.x + g.xmax, pk.pos.y + g.ymax, pk.pos.z + g.zmax}, ci, cj, ck);
             if (ci < 1 || cj < 1 || ck < 1) {
                 pk.tflag = true;
                 break;
@@ -1457,6 +1472,7 @@ int32_t oracle_run(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt
     A.pol.crossing_f64 = pol->crossing_f64 != 0;
     A.pol.kill_le = pol->ref_dda == 0;  // device semantics
     A.pol.near_f64 = pol->near_surface_f64 != 0;
+    A.pol.near_band = near_band(grid, pol->eps);
     A.pol.max_steps = pol->max_trace_steps > 0 ? pol->max_trace_steps : 1000000;
     A.first = first;
     A.count = count;
@@ -1522,6 +1538,7 @@ int32_t oracle_adjoint(const smcrt_scene* scene, const smcrt_grid* grid, const s
     A.pol.crossing_f64 = pol->crossing_f64 != 0;
     A.pol.kill_le = pol->ref_dda == 0;
     A.pol.near_f64 = pol->near_surface_f64 != 0;
+    A.pol.near_band = near_band(grid, pol->eps);
     A.pol.max_steps = pol->max_trace_steps > 0 ? pol->max_trace_steps : 1000000;
     A.first = 0;
     A.count = nphotons;
@@ -1651,11 +1668,8 @@ int32_t oracle_emit(const smcrt_scene* scene, const smcrt_grid* grid, const smcr
     // near-surface FP64 rule and the FP32 default epsilon, or FP64
     Pol pol{};
     pol.near_f64 = precision == SMCRT_FP32;
-    {
-        int e;
-        std::frexp(std::max(grid->xmax, std::max(grid->ymax, grid->zmax)), &e);
-        pol.eps = precision == SMCRT_FP32 ? std::max(1e-8, 8.0 * std::ldexp(1.0, e - 24)) : 1e-8;
-    }
+    pol.eps = 1e-8;
+    pol.near_band = near_band(grid, pol.eps);
     const Scene<double> sc64 = make_scene<double>(scene);
     for (int64_t q = 0; q < npk; ++q) {
         if (precision == SMCRT_FP32) {

@@ -190,13 +190,20 @@ int fill_dets(DetT* out, const smcrt_detector* dets, int ndet, int nregions, lon
     return SMCRT_OK;
 }
 
-double default_eps(int precision, const smcrt_grid& g) {
-    if (precision == SMCRT_FP64) return 1e-8;
-    double L = std::fmax(g.xmax, std::fmax(g.ymax, g.zmax));
+// Surface epsilon: the reference's 1e-8 (src/inttau2.f90:44) in both precisions.
+// FP32 transport can keep it because every decision against it is taken in FP64
+// (sweeps within near_band of a surface and crossing sweeps, see the kernel).
+double default_eps(int, const smcrt_grid&) { return 1e-8; }
+
+// FP32 transport: the distance below which a sweep is repeated in FP64 -- 16 FP32
+// ulps of the largest grid half-size (FP32 coordinate rounding and the affine
+// transform move a distance by a few ulps), and at least twice eps.
+double near_band(double eps, const smcrt_grid& g) {
+    const double L = std::fmax(g.xmax, std::fmax(g.ymax, g.zmax));
     int e;
-    std::frexp(L, &e);                  // L in [2^(e-1), 2^e)
-    double ulp = std::ldexp(1.0, e - 24);  // FP32 spacing at L
-    return std::fmax(1e-8, 8.0 * ulp);
+    std::frexp(L, &e);                     // L in [2^(e-1), 2^e)
+    const double ulp = std::ldexp(1.0, e - 24);  // FP32 spacing at L
+    return std::fmax(2.0 * eps, 16.0 * ulp);
 }
 
 int pick_device(int& dev, int& nsm) {
@@ -332,6 +339,7 @@ void fill_params(Params<R>* P, const smcrt_scene* scene, const smcrt_grid* grid,
     P->max_steps = (o && o->max_trace_steps > 0) ? o->max_trace_steps : 1000000;
     const int prec = (sizeof(R) == 4) ? SMCRT_FP32 : SMCRT_FP64;
     P->eps = (R)((o && o->eps > 0) ? o->eps : default_eps(prec, *grid));
+    P->near_band = (R)near_band((double)P->eps, *grid);
     P->normal_h = (o && o->normal_h > 0) ? o->normal_h : 1e-6;
     P->instance = o ? o->instance : 0u;
     P->tcopies = 1;

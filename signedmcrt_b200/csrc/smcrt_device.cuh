@@ -534,6 +534,7 @@ struct Params {
     int end_early;
     int max_steps;
     R eps;
+    R near_band;  // FP32 transport: sweeps closer than this to a surface are taken in FP64
     double normal_h;
     unsigned long long seed;
     unsigned long long budget_ns;  // per-launch device time budget (0 = none)

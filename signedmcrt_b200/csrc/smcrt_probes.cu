@@ -202,11 +202,11 @@ __global__ void k_emit(const __grid_constant__ Params<R> P, long long first, lon
     Stream<R, false> rng;
     rng.init(P.seed, P.instance, (uint64_t)(first + i), nullptr, 0);
     emit(P, pk, rng);
-    // the launch sweep as the transport kernel takes it: within 2 eps of a
+    // the launch sweep as the transport kernel takes it: within near_band of a
     // surface, FP32 transport decides on the FP64 position with the FP64 scene
     const SweepOut<R> o = sweep_regions<R, true>(P.sc, cv<R>(pk.pos), 0);
     int lay = o.lay;
-    if (sizeof(R) == 4 && o.mna <= (R)2 * P.eps) lay = sweep_regions<double, true>(P.sc64, pk.pos, 0).lay;
+    if (sizeof(R) == 4 && o.mna <= P.near_band) lay = sweep_regions<double, true>(P.sc64, pk.pos, 0).lay;
     layer[i] = lay + 1;
     pos[3 * i] = pk.pos.x;
     pos[3 * i + 1] = pk.pos.y;

@@ -275,7 +275,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #endif
 
 // Per-lane actions of the flattened transport loop.
-// A_PRECISE (FP32 transport): a sweep within 2 eps of a surface, or resolving a
+// A_PRECISE (FP32 transport): a sweep within the FP64 band of a surface, or resolving a
 // crossing, deferred to the next round and done in FP64 with the other such packets.
 enum Act : int { A_NEW = 0, A_SWEEP, A_WALK, A_CROSS, A_INTERACT, A_DEATH, A_DONE, A_PRECISE };
 // What the next sweep is for.
@@ -363,13 +363,6 @@ __device__ __forceinline__ V3<double> calc_normal_cold(const S& sc, int r, V3<do
     return calc_normal<MODS, S>(sc, r, p, h);
 }
 
-// Step start in grid coordinates (the position does not move during a walk).
-template <class R>
-__device__ __forceinline__ V3<R> grid_origin(const GridT<R>& g, const V3<double>& pos) {
-    const V3<R> p = cv<R>(pos);
-    return V3<R>{p.x + g.xmax, p.y + g.ymax, p.z + g.zmax};
-}
-
 // Starts a sphere-tracing step of length f.dsdf (body of the while loop at
 // inttau2.f90:63-83): optical depth bookkeeping, then the voxel-walk setup.
 // Returns A_WALK, or -1 when the step starts outside the grid (no tally).
@@ -387,24 +380,30 @@ __device__ __forceinline__ int start_step(const Params<R>& P, const Pk<R>& pk, F
         f.last = true;
     }
     const GridT<R>& g = P.grid;
-    const V3<R> o = grid_origin(g, pk.pos);
-    f.w.ci = (int)floor((R)g.nx * o.x / ((R)2 * g.xmax)) + 1;
-    f.w.cj = (int)floor((R)g.ny * o.y / ((R)2 * g.ymax)) + 1;
-    f.w.ck = (int)floor((R)g.nz * o.z / ((R)2 * g.zmax)) + 1;
+    // the start cell and the distances to its faces from the FP64 position: an FP32
+    // coordinate within an ulp of a grid face can round onto it, and a packet that
+    // stopped eps inside the grid's outer face would then start outside the grid
+    const double ox = pk.pos.x + g.xmax_d, oy = pk.pos.y + g.ymax_d, oz = pk.pos.z + g.zmax_d;
+    f.w.ci = (int)floor((double)g.nx * ox / (2.0 * g.xmax_d)) + 1;
+    f.w.cj = (int)floor((double)g.ny * oy / (2.0 * g.ymax_d)) + 1;
+    f.w.ck = (int)floor((double)g.nz * oz / (2.0 * g.zmax_d)) + 1;
     if (f.w.ci < 1 || f.w.ci > g.nx || f.w.cj < 1 || f.w.cj > g.ny || f.w.ck < 1 || f.w.ck > g.nz) {
         tflag = true;  // outside the grid: no tally for this step
         return -1;
     }
     // distance to the first face on each axis, then one face spacing per crossing
     // (Amanatides & Woo): no division per segment
+    // (the faces at FP64 multiples of the FP64 voxel size: the FP32 voxel size
+    // times a cell index misplaces the grid's outer face by tens of eps)
     const R big = (R)1e30;
     const V3<R>& d = pk.dir;
-    f.w.tx = d.x > (R)0 ? fmax(((R)f.w.ci * g.vx - o.x) / d.x, (R)0)
-           : d.x < (R)0 ? fmax(((R)(f.w.ci - 1) * g.vx - o.x) / d.x, (R)0) : big;
-    f.w.ty = d.y > (R)0 ? fmax(((R)f.w.cj * g.vy - o.y) / d.y, (R)0)
-           : d.y < (R)0 ? fmax(((R)(f.w.cj - 1) * g.vy - o.y) / d.y, (R)0) : big;
-    f.w.tz = d.z > (R)0 ? fmax(((R)f.w.ck * g.vz - o.z) / d.z, (R)0)
-           : d.z < (R)0 ? fmax(((R)(f.w.ck - 1) * g.vz - o.z) / d.z, (R)0) : big;
+    const double vx = 2.0 * g.xmax_d / g.nx, vy = 2.0 * g.ymax_d / g.ny, vz = 2.0 * g.zmax_d / g.nz;
+    f.w.tx = d.x > (R)0 ? fmax((R)((double)f.w.ci * vx - ox) / d.x, (R)0)
+           : d.x < (R)0 ? fmax((R)((double)(f.w.ci - 1) * vx - ox) / d.x, (R)0) : big;
+    f.w.ty = d.y > (R)0 ? fmax((R)((double)f.w.cj * vy - oy) / d.y, (R)0)
+           : d.y < (R)0 ? fmax((R)((double)(f.w.cj - 1) * vy - oy) / d.y, (R)0) : big;
+    f.w.tz = d.z > (R)0 ? fmax((R)((double)f.w.ck * vz - oz) / d.z, (R)0)
+           : d.z < (R)0 ? fmax((R)((double)(f.w.ck - 1) * vz - oz) / d.z, (R)0) : big;
     f.w.td = 0;
     return A_WALK;
 }
@@ -748,10 +747,11 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         if (KERNEL == SMCRT_KERNEL_WEIGHT) {
             const R wa = pk.weight * ((R)1 - albedo);
             pk.weight = pk.weight - wa;
-            const R ox = (R)pk.pos.x + P.grid.xmax, oy = (R)pk.pos.y + P.grid.ymax, oz = (R)pk.pos.z + P.grid.zmax;
-            const int ci = (int)floor((R)P.grid.nx * ox / ((R)2 * P.grid.xmax)) + 1;
-            const int cj = (int)floor((R)P.grid.ny * oy / ((R)2 * P.grid.ymax)) + 1;
-            const int ck = (int)floor((R)P.grid.nz * oz / ((R)2 * P.grid.zmax)) + 1;
+            // the interaction's voxel from the FP64 position (see start_step)
+            const double ox = pk.pos.x + P.grid.xmax_d, oy = pk.pos.y + P.grid.ymax_d, oz = pk.pos.z + P.grid.zmax_d;
+            const int ci = (int)floor((double)P.grid.nx * ox / (2.0 * P.grid.xmax_d)) + 1;
+            const int cj = (int)floor((double)P.grid.ny * oy / (2.0 * P.grid.ymax_d)) + 1;
+            const int ck = (int)floor((double)P.grid.nz * oz / (2.0 * P.grid.zmax_d)) + 1;
             if (ci < 1 || ci > P.grid.nx || cj < 1 || cj > P.grid.ny || ck < 1 || ck > P.grid.nz) {
                 pk.tflag = true;
                 act = A_DEATH;
@@ -803,12 +803,14 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         }
     }
     // ---- evaluate every region at the current position (the one inlined sweep)
-    // Within 2 eps of a surface, or resolving a crossing, FP32 transport takes the
-    // decisions (surface reached, crossing step, new region, the kill at a flight's
-    // start) on the FP64 position with the FP64 scene: an FP32 coordinate near 1 cm
-    // is only good to ~1e-7 cm, a tenth of eps, and that noise changed how many
-    // refracted packets the eps rule kills (-0.8% fluence).  Such sweeps are
-    // deferred as A_PRECISE so that they run together, not one lane per warp.
+    // Within near_band of a surface (16 FP32 ulps of the scene size, where FP32
+    // coordinate rounding could move a distance across eps), or resolving a
+    // crossing, FP32 transport takes the decisions (surface reached, crossing step,
+    // new region, the kill at a flight's start) on the FP64 position with the FP64
+    // scene, against the reference's eps: FP32 coordinates near 1 cm are only good
+    // to ~1e-7 cm, ten times eps, and that noise changed how many refracted packets
+    // the eps rule kills (-0.8% fluence).  Such sweeps are deferred as A_PRECISE so
+    // that they run together, not one lane per warp.
     if (act == A_SWEEP || act == A_PRECISE) {
         const int L = pk.layer;
         SweepOut<R> sw;
@@ -819,7 +821,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             precise = true;
         } else {
             sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L);
-            defer = sizeof(R) == 4 && (sw.mna <= (R)2 * eps || f.mode == S_CROSS);
+            defer = sizeof(R) == 4 && (sw.mna <= P.near_band || f.mode == S_CROSS);
         }
         if (defer) {
             act = A_PRECISE;
@@ -977,42 +979,17 @@ struct SlotCount {
     static constexpr int per_thread = sizeof(R) == 4 ? SMCRT_SLOTS_PER_THREAD : 1;
     static constexpr int n = kBlock * per_thread;
 };
-// Work queues of the actions a packet can wait in between passes, in the order
-// a warp looks for a full chunk of 32: FP64 near-surface sweep, retire/launch,
-// interact, sweep (or a pending crossing), walk.  The rare actions come first
-// so that they are taken as soon as 32 of them wait, and the common ones hold
-// the rest of the CTA's packets.  A_DONE maps to kGroups (never queued).
-// Nibble `act` of SMCRT_GROUP_ORDER is the queue of action `act`.
-#ifndef SMCRT_SCHED
-#define SMCRT_SCHED 2
-#endif
+// Sort groups of the actions a packet can wait in between rounds, in list
+// order: FP64 near-surface sweep, sweep (or a pending crossing), walk, interact,
+// retire/launch.  Each warp's first chunk is fixed (warp w, chunk w), so the
+// costly FP64 chunks at the head of the list go to different warps; the rest of
+// the list goes to whichever warp finishes first.  A_DONE maps to kGroups (not
+// listed).  Nibble `act` of SMCRT_GROUP_ORDER is the group of action `act`.
 #ifndef SMCRT_GROUP_ORDER
-#if SMCRT_SCHED == 0
 #define SMCRT_GROUP_ORDER 0x05431214u
-#else
-#define SMCRT_GROUP_ORDER 0x05123431u
-#endif
 #endif
 constexpr int kGroups = 5;
 __device__ __forceinline__ int act_group(int act) { return (int)((SMCRT_GROUP_ORDER >> (4 * act)) & 0xFu); }
-// Ring capacity of one queue: a power of two of at least the slots of a CTA (a
-// slot sits in at most one queue, so no queue ever holds more than that).
-constexpr int kQueueCap = 2048;
-// Bank-aligned queues: per action and bank, a ring of kSubCap slot indices (at
-// least the slots of one bank, SlotCount<R>::n / 32); a chunk is taken when at
-// least kChunkFull lanes find an entry.
-constexpr int kSubCap = 64;
-#ifndef SMCRT_CHUNK_FULL
-#define SMCRT_CHUNK_FULL 24
-#endif
-constexpr int kChunkFull = SMCRT_CHUNK_FULL;
-constexpr unsigned short kQueueEmpty = 0xFFFFu;
-static_assert(SlotCount<float>::n <= kQueueCap && SlotCount<double>::n <= kQueueCap, "queue ring too small");
-static_assert(SlotCount<float>::n < kQueueEmpty, "slot index collides with the empty mark");
-static_assert(SlotCount<float>::n / 32 <= kSubCap && SlotCount<float>::n % 32 == 0 && SlotCount<double>::n % 32 == 0,
-              "bank rings too small");
-static_assert(kGroups * kSubCap * 32 <= kGroups * kQueueCap, "bank rings exceed the queue area");
-
 template <class R, bool ADJ, int kSlots = SlotCount<R>::n>
 struct Slots {
     static constexpr int kRW = sizeof(R) / 4;  // 32-bit words per R
@@ -1173,47 +1150,25 @@ __device__ __forceinline__ void store_slot(Slots<R, ADJ>& sl, int s, int act, co
     }
 }
 
-// Dynamic shared memory of one CTA: the slots, the work-queue rings, then the
-// privatized detector bins.
-constexpr size_t kQueueBytes = sizeof(unsigned short) * kGroups * kQueueCap;
+// Dynamic shared memory of one CTA: the slots, then the privatized detector bins.
 template <class R, bool ADJ = false>
 __host__ __device__ constexpr size_t slots_bytes() {
-    return (sizeof(Slots<R, ADJ>) + 15) / 16 * 16 + kQueueBytes;
+    return (sizeof(Slots<R, ADJ>) + 15) / 16 * 16;
 }
-
-__device__ __forceinline__ unsigned vload(const unsigned* p) { return *(const volatile unsigned*)p; }
-__device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
-
-// Spin limits of the scheduler's waits.  A queue entry is written a few
-// instructions after its place is claimed, so its wait is short; the idle wait
-// of a warp that finds every queue empty lasts until other warps push work, and
-// is bounded by the launch's time budget (and by this count when there is none).
-constexpr int kEntrySpinLimit = 1 << 22;
-constexpr unsigned kIdleSpinLimit = 1u << 31;
 
 // The persistent, compacted kernel.  KERNEL: smcrt_kernel_kind.  REPLAY:
 // injected streams.
 //
-// A CTA holds SlotCount<R>::n packets in shared-memory slots.  Each slot waits
-// in one of kGroups work queues (rings of slot indices in shared memory), the
-// queue of the action its packet does next.  A warp takes a chunk of up to 32
-// slots from one queue -- the first queue in priority order holding a full
-// chunk, else the fullest -- runs one pass of each packet's state machine, writes
-// the packets back and appends each slot to the queue of its next action.  A warp
-// therefore works on 32 packets that start the pass with the same action, and
-// rare actions (boundary events, retire and launch, the FP64 near-surface
-// sweeps) are gathered across the CTA instead of stalling 31 idle lanes.  The
-// warps run independently: no CTA barrier between passes, so a warp never waits
-// for the slowest chunk of the others.
-//
-// Queue protocol: a producer claims ring positions with an atomic add on the
-// queue's tail and writes each slot index there after the slot's data (a
-// block-scope fence in between); a consumer claims positions with a
-// compare-and-swap on the head, waits for each entry to leave the empty mark,
-// reads it and puts the mark back.  A slot is in at most one queue, so no ring
-// holds more than SlotCount<R>::n <= kQueueCap entries and a position is never
-// reused before its previous entry was consumed.  The kernel ends when every
-// slot has found no packet left to launch (or the time budget ran out).
+// A CTA holds SlotCount<R>::n packets in shared memory.  Each round it counting-sorts
+// its live slots by their next action (warp ballots, stable in slot order), then
+// the warps take 32-item chunks of the sorted list, run one pass of each packet's
+// state machine and write the packets back.  A warp therefore works on 32
+// packets that start the pass with the same action, whatever mix of actions the
+// CTA's packets are in; rare actions (boundary events, retire and launch) are
+// gathered across the CTA instead of stalling 31 idle lanes.  Chunks of a group
+// hold consecutive slots, so the structure-of-arrays slot accesses of a warp fall
+// in different shared-memory banks, and the warps of a round run the same
+// action's code at about the same time.
 // MODS = false compiles every distance evaluation without the modifier code,
 // for scenes whose primitives carry no modifiers.  BIG reads the scene from
 // device memory (scenes beyond the parameter block's kMaxRegions/kMaxPrims).
@@ -1224,11 +1179,9 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     constexpr int NS = SlotCount<R>::n;
     __shared__ unsigned long long s_cnt[C_NUM];
     __shared__ double s_mom[25];
-    __shared__ int s_done;  // slots with no packet left to launch
-    __shared__ int s_stop;  // the time budget ran out (or a wait gave up)
+    __shared__ int s_stop;  // the time budget ran out
     extern __shared__ __align__(16) unsigned char s_dyn[];
     Slots<R, ADJ>& sl = *reinterpret_cast<Slots<R, ADJ>*>(s_dyn);
-    unsigned char* s_qmem = s_dyn + slots_bytes<R, ADJ>() - kQueueBytes;
     unsigned* s_bins = reinterpret_cast<unsigned*>(s_dyn + slots_bytes<R, ADJ>());
     const int t = threadIdx.x;
     const unsigned lane = lane_id();
@@ -1236,10 +1189,6 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     if (t < 25) s_mom[t] = 0.0;
     for (int i = t; i < P.sbins; i += kBlock) s_bins[i] = 0u;
     for (int i = t; i < NS; i += kBlock) sl.meta[i] = (uint32_t)A_NEW;
-    if (t == 0) {
-        s_done = 0;
-        s_stop = 0;
-    }
     // adjoint: per-thread gradient accumulators [3][kMaxAdjGroups][kBlock]
     __shared__ float s_acc[ADJ ? 3 * kMaxAdjGroups * kBlock : 1];
     if (ADJ)
@@ -1255,9 +1204,6 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     // this CTA's voxel-score tables (second-moment runs)
     uint2* const vbase = VAR ? P.var_tab + (size_t)blockIdx.x * NS * kVarEntries : nullptr;
     const unsigned lt = (1u << lane) - 1u;
-    (void)lt;
-    (void)s_qmem;
-#if SMCRT_SCHED == 0
     // ---- rounds: each round counting-sorts the live slots by action (warp
     // ballots and a per-warp scan, stable in slot order) and the warps take
     // 32-item chunks of the sorted list; three CTA barriers a round
@@ -1344,188 +1290,6 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
             chunk = __shfl_sync(0xffffffffu, next, 0);
         }
     }
-#elif SMCRT_SCHED == 1
-    // ---- one ring per action; a warp claims up to 32 consecutive entries
-    __shared__ unsigned s_head[kGroups], s_tail[kGroups];
-    auto s_q = reinterpret_cast<unsigned short (*)[kQueueCap]>(s_qmem);
-    const int gnew = act_group(A_NEW);
-    for (int i = t; i < kGroups * kQueueCap; i += kBlock) {
-        const int g = i / kQueueCap, k = i % kQueueCap;
-        s_q[g][k] = (g == gnew && k < NS) ? (unsigned short)k : kQueueEmpty;
-    }
-    if (t < kGroups) {
-        s_head[t] = 0u;
-        s_tail[t] = (t == gnew) ? (unsigned)NS : 0u;
-    }
-    __syncthreads();
-    unsigned idle = 0;
-    for (;;) {
-        int g = -1, take = 0;
-        unsigned h = 0;
-        if (lane == 0) {
-            for (int tries = 0; tries < 256; ++tries) {
-                int best = -1, bavail = 0;
-                unsigned bh = 0;
-#pragma unroll
-                for (int k = 0; k < kGroups; ++k) {
-                    const unsigned hk = vload(&s_head[k]);
-                    const int av = (int)(vload(&s_tail[k]) - hk);
-                    if (av > bavail && bavail < 32) {
-                        best = k;
-                        bavail = av;
-                        bh = hk;
-                    }
-                }
-                if (best < 0) break;
-                const int n = bavail < 32 ? bavail : 32;
-                if (atomicCAS(&s_head[best], bh, bh + (unsigned)n) == bh) {
-                    g = best;
-                    h = bh;
-                    take = n;
-                    break;
-                }
-            }
-        }
-        take = __shfl_sync(0xffffffffu, take, 0);
-        if (take == 0) {
-            if (__any_sync(0xffffffffu, vload(&s_done) >= NS || vload(&s_stop))) break;
-            if (lane == 0 && ((P.budget_ns && global_ns() - t0 > P.budget_ns) || ++idle > kIdleSpinLimit)) {
-                atomicOr(B.status, STATUS_ABORTED);
-                s_stop = 1;
-            }
-            __syncwarp();
-            __nanosleep(200);
-            continue;
-        }
-        g = __shfl_sync(0xffffffffu, g, 0);
-        h = __shfl_sync(0xffffffffu, h, 0);
-        int s = -1, act = A_DONE;
-        if ((int)lane < take) {
-            volatile unsigned short* e = &s_q[g][(h + lane) & (unsigned)(kQueueCap - 1)];
-            unsigned short v = *e;
-            for (int spin = 0; v == kQueueEmpty && spin < kEntrySpinLimit; ++spin) v = *e;
-            if (v == kQueueEmpty) {
-                atomicOr(B.status, STATUS_ABORTED);
-                s_stop = 1;
-            } else {
-                *e = kQueueEmpty;
-                s = (int)v;
-            }
-        }
-        __threadfence_block();
-        if (s >= 0) {
-            act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
-                P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc, VAR ? vbase + (size_t)s * kVarEntries : nullptr);
-            store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
-        }
-        __threadfence_block();
-        const int grp = s >= 0 ? act_group(act) : kGroups;
-#pragma unroll
-        for (int k = 0; k < kGroups; ++k) {
-            const unsigned m = __ballot_sync(0xffffffffu, grp == k);
-            if (m) {
-                const int leader = __ffs(m) - 1;
-                unsigned base = 0;
-                if ((int)lane == leader) base = atomicAdd(&s_tail[k], (unsigned)__popc(m));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (grp == k)
-                    s_q[k][(base + (unsigned)__popc(m & lt)) & (unsigned)(kQueueCap - 1)] = (unsigned short)s;
-            }
-        }
-        const unsigned md = __ballot_sync(0xffffffffu, s >= 0 && act == A_DONE);
-        if (lane == 0) {
-            if (md) atomicAdd(&s_done, __popc(md));
-            if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
-                atomicOr(B.status, STATUS_ABORTED);
-                s_stop = 1;
-            }
-        }
-        if (__any_sync(0xffffffffu, vload(&s_stop) != 0)) break;
-    }
-#else
-    // ---- bank-aligned queues: slot s always waits in sub-queue (action, s mod 32)
-    // and is always run by lane s mod 32 of some warp, so a chunk's slot loads and
-    // stores hit 32 different shared-memory banks, and a lane pushes its slot
-    // without any warp-wide step.  A warp takes the head entry of its lanes'
-    // sub-queues of one action: the first action (in queue priority order) with
-    // at least kChunkFull lanes' worth waiting, else the one with the most.
-    __shared__ unsigned s_bh[kGroups][32], s_bt[kGroups][32];
-    auto s_q = reinterpret_cast<unsigned short (*)[kSubCap][32]>(s_qmem);  // [group][position][bank]
-    const int gnew = act_group(A_NEW);
-    for (int i = t; i < kGroups * kSubCap * 32; i += kBlock) {
-        const int g = i / (kSubCap * 32), k = (i / 32) % kSubCap, b = i % 32;
-        s_q[g][k][b] = (g == gnew && k < NS / 32) ? (unsigned short)(b + 32 * k) : kQueueEmpty;
-    }
-    if (t < kGroups * 32) {
-        s_bh[t / 32][t % 32] = 0u;
-        s_bt[t / 32][t % 32] = (t / 32 == gnew) ? (unsigned)(NS / 32) : 0u;
-    }
-    __syncthreads();
-    unsigned idle = 0;
-    for (;;) {
-        int g = -1, bestn = 0;
-#pragma unroll
-        for (int k = 0; k < kGroups; ++k) {
-            const bool has = vload(&s_bt[k][lane]) != vload(&s_bh[k][lane]);
-            const int n = __popc(__ballot_sync(0xffffffffu, has));
-            if (n > bestn && bestn < kChunkFull) {
-                g = k;
-                bestn = n;
-            }
-        }
-        if (g < 0) {
-            if (__any_sync(0xffffffffu, vload(&s_done) >= NS || vload(&s_stop))) break;
-            if (lane == 0 && ((P.budget_ns && global_ns() - t0 > P.budget_ns) || ++idle > kIdleSpinLimit)) {
-                atomicOr(B.status, STATUS_ABORTED);
-                s_stop = 1;
-            }
-            __syncwarp();
-            __nanosleep(200);
-            continue;
-        }
-        int s = -1, act = A_DONE;
-        for (int tries = 0; tries < 8; ++tries) {
-            const unsigned h = vload(&s_bh[g][lane]);
-            if (vload(&s_bt[g][lane]) == h) break;  // this lane's sub-queue is empty now
-            if (atomicCAS(&s_bh[g][lane], h, h + 1u) == h) {
-                volatile unsigned short* e = &s_q[g][h & (unsigned)(kSubCap - 1)][lane];
-                unsigned short v = *e;
-                for (int spin = 0; v == kQueueEmpty && spin < kEntrySpinLimit; ++spin) v = *e;
-                if (v == kQueueEmpty) {  // never written: give up on this slot and stop the CTA
-                    atomicOr(B.status, STATUS_ABORTED);
-                    s_stop = 1;
-                } else {
-                    *e = kQueueEmpty;
-                    s = (int)v;
-                }
-                break;
-            }
-        }
-        __threadfence_block();  // the slot's data was written before its entry
-        if (s >= 0) {
-            act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-            transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
-                P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc, VAR ? vbase + (size_t)s * kVarEntries : nullptr);
-            store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
-        }
-        __threadfence_block();  // the slot's data before the entry that publishes it
-        if (s >= 0 && act != A_DONE) {
-            const int k = act_group(act);
-            const unsigned pos = atomicAdd(&s_bt[k][lane], 1u);
-            s_q[k][pos & (unsigned)(kSubCap - 1)][lane] = (unsigned short)s;
-        }
-        const unsigned md = __ballot_sync(0xffffffffu, s >= 0 && act == A_DONE);
-        if (lane == 0) {
-            if (md) atomicAdd(&s_done, __popc(md));
-            if (P.budget_ns && global_ns() - t0 > P.budget_ns) {
-                atomicOr(B.status, STATUS_ABORTED);
-                s_stop = 1;
-            }
-        }
-        if (__any_sync(0xffffffffu, vload(&s_stop) != 0)) break;
-    }
-#endif
     // events of packets still in flight (time budget) and since the last retire
     atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);
     atomicAdd(&s_cnt[C_VOX], (unsigned long long)c.vox);

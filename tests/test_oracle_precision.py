@@ -1,6 +1,6 @@
-"""The FP32 device semantics (the GPU's FP32 kernels' algorithm: epsilon
-max(1e-8, 8 ulp), integer voxel walk, FP64 boundary events, and sweeps within
-2 eps of a surface or after a crossing step in FP64) against the reference
+"""The FP32 device semantics (the GPU's FP32 kernels' algorithm: the reference's
+epsilon 1e-8, integer voxel walk, FP64 boundary events, and sweeps within 16 FP32
+ulps of a surface or after a crossing step in FP64) against the reference
 semantics (FP64, eps 1e-8, the snapping voxel walk of src/inttau2.f90:213-441),
 both in the CPU oracle, on the curved refracting surface of sphere_water: the
 epsilon policy must not move the fluence, the total path length, or the rates
