@@ -471,7 +471,12 @@ def run_adjoint(args) -> None:
                          "fd_se": dict(zip(names, (fd.std(axis=0, ddof=1) / np.sqrt(B)).tolist())),
                          "fd_informative": dict(zip(names, informative.tolist())),
                          "within_2sigma": int((np.abs(z[informative]) < 2).sum()),
-                         "informative": int(informative.sum())},
+                         "within_3sigma": int((np.abs(z[informative]) < 3).sum()),
+                         "max_abs_z": float(np.abs(z[informative]).max()) if informative.any() else None,
+                         "mean_z2": float(np.mean(z[informative] ** 2)) if informative.any() else None,
+                         "informative": int(informative.sum()),
+                         "sigma": "standard error of the difference of the batch means (adjoint and CRN finite "
+                                  "differences), each from the spread of its batches"},
             "gpu_launches": 2 * args.steps}
     print(json.dumps(line), flush=True)
 
@@ -491,6 +496,7 @@ def main() -> None:
     ap.add_argument("--batch-scale", type=float, default=1.0, help="batch256: packet counts x this factor")
     ap.add_argument("--packets", type=float, default=0, help="packets per GPU per step (default: the config's)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--eps", type=float, default=0.0, help="surface epsilon (default: the library's, 1e-8)")
     ap.add_argument("--num-spheres", type=int, default=40,
                     help="sphere_scene: spheres of the reference's res/sphere.toml scene (regions = this + 1)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample length")
@@ -552,7 +558,8 @@ def main() -> None:
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)  # every timed launch goes to this stream
     torch.cuda.set_stream(stream)
-    tr = T.Transport(flat, st, precision=args.precision, stream=stream.cuda_stream, timeout_ms=600000)
+    tr = T.Transport(flat, st, precision=args.precision, stream=stream.cuda_stream, timeout_ms=600000,
+                     eps=args.eps)
     jm = torch.zeros(tr.ncell, dtype=torch.float64, device=dev)
     bins = torch.zeros(max(tr.nbins, 1), dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
@@ -607,7 +614,7 @@ def main() -> None:
     if not args.no_e2e:
         jh = torch.empty(tr.ncell, dtype=torch.float64, pin_memory=True).numpy()
         bh = torch.empty(max(tr.nbins, 1), dtype=torch.float64, pin_memory=True).numpy()
-        tr_host = T.Transport(flat, st, precision=args.precision, timeout_ms=600000)
+        tr_host = T.Transport(flat, st, precision=args.precision, timeout_ms=600000, eps=args.eps)
         tr_host.run(min(per_gpu, 100000), 1, jmean_out=jh, bins_out=bh[:tr_host.nbins] if tr_host.nbins else None)
         if world > 1:
             dist.barrier()

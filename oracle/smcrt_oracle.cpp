@@ -484,6 +484,21 @@ inline void voxel_of(const GridD& g, V3<R> p, int& ci, int& cj, int& ck) {
     if (cj > g.ny || cj < 1) cj = -1;
     if (ck > g.nz || ck < 1) ck = -1;
 }
+// The device semantics' cell of an FP64 grid-coordinate point: FP64 transport
+// divides as update_voxels does; FP32 transport multiplies by the FP64 n / (2 max).
+template <class R>
+inline void cell_of(const GridD& g, V3<double> p, int& ci, int& cj, int& ck) {
+    if (sizeof(R) == 8) {
+        voxel_of(g, p, ci, cj, ck);
+        return;
+    }
+    ci = (int)std::floor(p.x * ((double)g.nx / (2.0 * g.xmax))) + 1;
+    cj = (int)std::floor(p.y * ((double)g.ny / (2.0 * g.ymax))) + 1;
+    ck = (int)std::floor(p.z * ((double)g.nz / (2.0 * g.zmax))) + 1;
+    if (ci > g.nx || ci < 1) ci = -1;
+    if (cj > g.ny || cj < 1) cj = -1;
+    if (ck > g.nz || ck < 1) ck = -1;
+}
 inline int64_t cell_index(const GridD& g, int i, int j, int k) {
     return (int64_t)(i - 1) + (int64_t)g.nx * ((int64_t)(j - 1) + (int64_t)g.ny * (int64_t)(k - 1));
 }
@@ -562,7 +577,7 @@ template <class R>
 bool update_grids_int(const GridD& g, V3<double> pos, V3<R> dir, R dsdf, Tally& t, Counters& c, bool& tflag) {
     const V3<double> o{pos.x + g.xmax, pos.y + g.ymax, pos.z + g.zmax};
     int ci, cj, ck;
-    voxel_of(g, o, ci, cj, ck);
+    cell_of<R>(g, o, ci, cj, ck);
     if (ci == -1 || cj == -1 || ck == -1) {
         tflag = true;
         return true;
@@ -1237,7 +1252,7 @@ void run_packet(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, c
             R wa = pk.weight * ((R)1 - rg.albedo);
             pk.weight = pk.weight - wa;
             int ci, cj, ck;
-            voxel_of(g, V3<double>{pk.pos.x + g.xmax, pk.pos.y + g.ymax, pk.pos.z + g.zmax}, ci, cj, ck);
+            cell_of<R>(g, V3<double>{pk.pos.x + g.xmax, pk.pos.y + g.ymax, pk.pos.z + g.zmax}, ci, cj, ck);
             if (ci < 1 || cj < 1 || ck < 1) {
                 pk.tflag = true;
                 break;

@@ -101,6 +101,9 @@ void fill_grid(GridT<R>& g, const smcrt_grid& s) {
     g.xmax_d = s.xmax;
     g.ymax_d = s.ymax;
     g.zmax_d = s.zmax;
+    g.sx_d = (double)s.nxg / (2.0 * s.xmax);
+    g.sy_d = (double)s.nyg / (2.0 * s.ymax);
+    g.sz_d = (double)s.nzg / (2.0 * s.zmax);
 }
 
 template <class R>
@@ -265,8 +268,9 @@ struct smcrt_ctx {
     bool big = false;                         // scene tables in device memory (d_scene)
     void* d_scene = nullptr;
     bool variance = false;                    // second-moment runs available
-    uint2* d_vartab = nullptr;                // voxel-score table of every packet slot
+    unsigned char* d_vartab = nullptr;        // voxel-score table of every packet slot
     size_t vartab_bytes = 0;
+    bool vartab_clean = false;                // every table seen empty after the last moments run
     double* d_jmean2 = nullptr;               // second moment of smcrt_run_moments
 };
 
@@ -394,12 +398,15 @@ void set_tally_table(Params<R>* P, double* jm, double* copies, int tc, long long
 }
 
 // Enqueues: reset work/counters/status, then the kernel for [first, first+count).
-// jm2: the second-moment grid of a moments run (nullptr otherwise); its voxel-score
-// tables are emptied first (a run stopped by its time budget leaves entries).
+// jm2: the second-moment grid of a moments run (nullptr otherwise).  Retiring
+// packets empty their voxel-score tables, so the tables are filled with the empty
+// key only before the first moments run and after one that was not seen to finish
+// (stopped by its time budget, or launched without a wait on its stats).
 int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, double* jm, double* bins, bool replay,
             const double* d_u, const long long* d_off, smcrt_packet_state* d_states, double* jm2 = nullptr) {
     CK(cudaMemsetAsync(c->d_work, 0, sizeof(unsigned long long) * (1 + C_NUM), c->stream));
-    if (jm2) CK(cudaMemsetAsync(c->d_vartab, 0xFF, c->vartab_bytes, c->stream));
+    if (jm2 && !c->vartab_clean) CK(cudaMemsetAsync(c->d_vartab, 0xFF, c->vartab_bytes, c->stream));
+    if (jm2) c->vartab_clean = false;
     CK(cudaMemsetAsync(c->d_mom, 0, sizeof(double) * 25, c->stream));
     CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
     Buffers B = make_buffers(c, jm, bins);
@@ -670,7 +677,7 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
                                                 std::to_string(kMaxPrims) + " primitives)"));
         c->variance = true;
         const size_t slots = (size_t)(prec == SMCRT_FP64 ? SlotCount<double>::n : SlotCount<float>::n);
-        c->vartab_bytes = sizeof(uint2) * (size_t)kVarEntries * slots * (size_t)c->grid_blocks;
+        c->vartab_bytes = kVarSlotBytes * slots * (size_t)c->grid_blocks;
         if (cudaMalloc(&c->d_vartab, c->vartab_bytes) != cudaSuccess)
             return bail(fail(SMCRT_ERR_CUDA, "variance: cannot allocate " + std::to_string(c->vartab_bytes >> 20) +
                                                  " MiB of voxel-score tables"));
@@ -885,6 +892,7 @@ int32_t smcrt_run_moments(smcrt_ctx* c, int64_t nphotons, uint64_t seed, double*
         CK(cudaMemcpyAsync(det_bins, c->d_bins, sizeof(double) * c->nbins, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     rc = read_stats(c, stats);
+    if (rc == SMCRT_OK) c->vartab_clean = true;
     if (stats)
         stats->d2h_bytes += (jmean ? sizeof(double) * (size_t)c->ncell : 0) +
                             (jmean2 ? sizeof(double) * (size_t)c->ncell : 0) +
@@ -908,7 +916,9 @@ int32_t smcrt_run_device_moments(smcrt_ctx* c, int64_t first, int64_t count, uin
     if (!stats) return SMCRT_OK;
     rc = wait_bounded(c);
     if (rc) return rc;
-    return read_stats(c, stats);
+    rc = read_stats(c, stats);
+    if (rc == SMCRT_OK) c->vartab_clean = true;
+    return rc;
 }
 
 int32_t smcrt_replay(smcrt_ctx* c, const double* uniforms, const int64_t* offsets, int64_t npackets, double* jmean,

@@ -499,6 +499,7 @@ struct GridT {
     R vx, vy, vz;       // voxel sizes 2*max/n
     R sx, sy, sz;       // n/(2*max) as written: n * p / (2 * max)
     double xmax_d, ymax_d, zmax_d;  // exact half sizes (grid-exit test on FP64 positions)
+    double sx_d, sy_d, sz_d;        // n / (2 max) in FP64 (FP32 transport's cell index of an FP64 position)
 };
 
 struct DetT {
@@ -564,9 +565,10 @@ struct Params {
     int adj_ngroups;
     unsigned char adj_group[kMaxRegions];
     // second-moment runs (the VAR instantiation): each packet slot's voxel-score
-    // table (kVarEntries (voxel, score) pairs, slot-major over the persistent
-    // grid's CTAs) and the per-voxel sum of squared per-packet scores
-    uint2* var_tab;
+    // table (kVarSlotBytes each: (voxel, score) pairs, the used list and its
+    // count; slot-major over the persistent grid's CTAs) and the per-voxel sum of
+    // squared per-packet scores
+    unsigned char* var_tab;
     double* jmean2;
 };
 

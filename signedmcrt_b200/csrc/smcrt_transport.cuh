@@ -63,7 +63,10 @@ struct Pk {
     int flags;
     int inst;  // batch instance (0 outside batches)
     int phase;        // adjoint: 0 = first pass (sum C), 1 = second pass (gradient terms)
-    float ctot, cpre; // adjoint: the packet's loss contribution C, and the part of it made so far
+    // adjoint: the packet's loss contribution C, and the part of it made so far, in
+    // FP64: their difference (the contribution still to come) cancels along
+    // histories of hundreds of segments
+    double ctot, cpre;
     bool tflag;
 };
 
@@ -363,6 +366,25 @@ __device__ __forceinline__ V3<double> calc_normal_cold(const S& sc, int r, V3<do
     return calc_normal<MODS, S>(sc, r, p, h);
 }
 
+// 1-based cell of a point given in FP64 grid coordinates (position + half size),
+// update_voxels' index formula (src/inttau2.f90:433-435): FP64 transport divides
+// as the reference does; FP32 transport multiplies by the FP64 n / (2 max) (an
+// FP64 division costs tens of instructions, and FP32 transport's walk is
+// statistically, not bitwise, the reference's).
+template <class R>
+__device__ __forceinline__ void cell_of(const GridT<R>& g, double ox, double oy, double oz, int& ci, int& cj,
+                                        int& ck) {
+    if (sizeof(R) == 8) {
+        ci = (int)floor((double)g.nx * ox / (2.0 * g.xmax_d)) + 1;
+        cj = (int)floor((double)g.ny * oy / (2.0 * g.ymax_d)) + 1;
+        ck = (int)floor((double)g.nz * oz / (2.0 * g.zmax_d)) + 1;
+    } else {
+        ci = (int)floor(ox * g.sx_d) + 1;
+        cj = (int)floor(oy * g.sy_d) + 1;
+        ck = (int)floor(oz * g.sz_d) + 1;
+    }
+}
+
 // Starts a sphere-tracing step of length f.dsdf (body of the while loop at
 // inttau2.f90:63-83): optical depth bookkeeping, then the voxel-walk setup.
 // Returns A_WALK, or -1 when the step starts outside the grid (no tally).
@@ -384,9 +406,7 @@ __device__ __forceinline__ int start_step(const Params<R>& P, const Pk<R>& pk, F
     // coordinate within an ulp of a grid face can round onto it, and a packet that
     // stopped eps inside the grid's outer face would then start outside the grid
     const double ox = pk.pos.x + g.xmax_d, oy = pk.pos.y + g.ymax_d, oz = pk.pos.z + g.zmax_d;
-    f.w.ci = (int)floor((double)g.nx * ox / (2.0 * g.xmax_d)) + 1;
-    f.w.cj = (int)floor((double)g.ny * oy / (2.0 * g.ymax_d)) + 1;
-    f.w.ck = (int)floor((double)g.nz * oz / (2.0 * g.zmax_d)) + 1;
+    cell_of<R>(g, ox, oy, oz, f.w.ci, f.w.cj, f.w.ck);
     if (f.w.ci < 1 || f.w.ci > g.nx || f.w.cj < 1 || f.w.cj > g.ny || f.w.ck < 1 || f.w.ck > g.nz) {
         tflag = true;  // outside the grid: no tally for this step
         return -1;
@@ -417,27 +437,52 @@ __device__ __forceinline__ R face_spacing(R v, R dcomp) {
 // ---------------------------------------------------------------------------
 // History-based second moment of the fluence tally.  The variance of a voxel's
 // tally needs each packet's own total score there (all of its segments in that
-// voxel added first), squared.  Every packet slot owns a table of kVarEntries
-// (voxel, score) pairs in device memory (open addressing, linear probing): a
-// segment adds into its voxel's entry, and the retiring packet adds each entry's
-// squared score to jmean2 and empties the table.  When kVarProbes probes find
-// neither the voxel nor a free entry, that one segment is squared on its own and
-// counted (C_VAROVF): the estimate then lacks the cross terms of that segment.
-constexpr int kVarLog2 = 9;
+// voxel added first), squared.  Every packet slot owns a table in device memory:
+// kVarEntries (voxel, score) pairs (open addressing, linear probing), the list of
+// the entries in use (16-bit positions, in the order they were taken) and their
+// count, stored complemented so that the all-ones fill of a fresh table reads as
+// zero.  A segment adds into its voxel's entry; the retiring packet adds each used
+// entry's squared score to jmean2 and empties it, so a retire costs the voxels the
+// packet visited, not the table size.  Probing runs until the voxel or a free
+// entry turns up; only a packet that visits more than kVarEntries distinct voxels
+// finds neither: that segment is squared on its own and counted (C_VAROVF), and the
+// estimate then lacks the cross terms of that segment.  (A 1-packet census of the
+// test scenes gives means of 80-240 distinct voxels and tails below 2000.)
+constexpr int kVarLog2 = 12;
 constexpr int kVarEntries = 1 << kVarLog2;
-constexpr int kVarProbes = 16;
 constexpr unsigned kVarEmpty = 0xFFFFFFFFu;
+// one slot's table: the pairs, the used list, the count (16-byte multiple)
+constexpr size_t kVarSlotBytes = (size_t)kVarEntries * 8 + (size_t)kVarEntries * 2 + 16;
+static_assert(kVarSlotBytes % 16 == 0, "slot tables keep 16-byte alignment");
 
-__device__ __forceinline__ void var_add(uint2* vt, double* jmean2, int idx, float v, Cnt& c) {
+struct VarTab {
+    uint2* e;
+    unsigned short* used;
+    unsigned* ncount;  // complement of the number of used entries
+};
+
+__device__ __forceinline__ VarTab var_table(unsigned char* base) {
+    VarTab t;
+    t.e = reinterpret_cast<uint2*>(base);
+    t.used = reinterpret_cast<unsigned short*>(base + (size_t)kVarEntries * 8);
+    t.ncount = reinterpret_cast<unsigned*>(base + (size_t)kVarEntries * 10);
+    return t;
+}
+
+__device__ __forceinline__ void var_add(unsigned char* vt, double* jmean2, int idx, float v, Cnt& c) {
+    const VarTab t = var_table(vt);
     unsigned h = ((unsigned)idx * 2654435761u) >> (32 - kVarLog2);
-    for (int k = 0; k < kVarProbes; ++k) {
-        const uint2 e = vt[h];
+    for (int k = 0; k < kVarEntries; ++k) {
+        const uint2 e = t.e[h];
         if (e.x == (unsigned)idx) {
-            vt[h].y = __float_as_uint(__uint_as_float(e.y) + v);
+            t.e[h].y = __float_as_uint(__uint_as_float(e.y) + v);
             return;
         }
         if (e.x == kVarEmpty) {
-            vt[h] = make_uint2((unsigned)idx, __float_as_uint(v));
+            t.e[h] = make_uint2((unsigned)idx, __float_as_uint(v));
+            const unsigned n = ~*t.ncount;
+            t.used[n] = (unsigned short)h;
+            *t.ncount = ~(n + 1u);
             return;
         }
         h = (h + 1u) & (unsigned)(kVarEntries - 1);
@@ -446,21 +491,17 @@ __device__ __forceinline__ void var_add(uint2* vt, double* jmean2, int idx, floa
     ++c.varovf;
 }
 
-__device__ __forceinline__ void var_flush(uint2* vt, double* jmean2) {
-    uint4* q = reinterpret_cast<uint4*>(vt);
-    for (int k = 0; k < kVarEntries / 2; ++k) {
-        const uint4 e = q[k];
-        if (e.x == kVarEmpty && e.z == kVarEmpty) continue;
-        if (e.x != kVarEmpty) {
-            const double sc = (double)__uint_as_float(e.y);
-            atomicAdd(jmean2 + e.x, sc * sc);
-        }
-        if (e.z != kVarEmpty) {
-            const double sc = (double)__uint_as_float(e.w);
-            atomicAdd(jmean2 + e.z, sc * sc);
-        }
-        q[k] = make_uint4(kVarEmpty, 0u, kVarEmpty, 0u);
+__device__ __forceinline__ void var_flush(unsigned char* vt, double* jmean2) {
+    const VarTab t = var_table(vt);
+    const unsigned n = ~*t.ncount;
+    for (unsigned k = 0; k < n; ++k) {
+        const unsigned h = t.used[k];
+        const uint2 e = t.e[h];
+        const double sc = (double)__uint_as_float(e.y);
+        atomicAdd(jmean2 + e.x, sc * sc);
+        t.e[h] = make_uint2(kVarEmpty, 0u);
     }
+    *t.ncount = kVarEmpty;
 }
 
 // One voxel segment of the current step; returns true when the step's walk is over.
@@ -468,7 +509,7 @@ __device__ __forceinline__ void var_flush(uint2* vt, double* jmean2) {
 // grid the rest of the step, untallied, still counts for survival.)
 template <class R, bool BATCH, bool ADJ, bool VAR>
 __device__ __forceinline__ bool walk_segment(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c, float* acc,
-                                             uint2* vt) {
+                                             unsigned char* vt) {
     const GridT<R>& g = P.grid;
     const V3<R>& d = pk.dir;
     const R tm = fmin(f.w.tx, fmin(f.w.ty, f.w.tz));
@@ -536,18 +577,18 @@ __device__ __forceinline__ void adj_add(float* acc, int k, int grp, float v) {
 template <class R>
 __device__ __forceinline__ void adj_track(const Params<R>& P, Pk<R>& pk, float* acc, float len, float w) {
     if (pk.phase == 0) {
-        pk.ctot += w * len;
+        pk.ctot += (double)(w * len);
         return;
     }
     const int grp = P.adj_group[pk.layer];
     if (grp < P.adj_ngroups) {
         // integral over the length of -(contributions after each point); the same
         // for mua and mus (d kappa / d mua = d kappa / d mus = 1)
-        const float v = len * (pk.ctot - pk.cpre) - 0.5f * w * len * len;
+        const float v = len * (float)(pk.ctot - pk.cpre) - 0.5f * w * len * len;
         adj_add(acc, 0, grp, -v);
         adj_add(acc, 1, grp, -v);
     }
-    pk.cpre += w * len;
+    pk.cpre += (double)(w * len);
 }
 
 // A scatter in the packet's region with HG variate mu (second pass).
@@ -556,7 +597,7 @@ __device__ __forceinline__ void adj_scatter(const Params<R>& P, const Pk<R>& pk,
     const int grp = P.adj_group[pk.layer];
     if (grp >= P.adj_ngroups) return;
     const DRegion<R>& rg = P.sc.region[pk.layer];
-    const float F = pk.ctot - pk.cpre;
+    const float F = (float)(pk.ctot - pk.cpre);
     if ((float)rg.mua < 1e-9f) {  // albedo 1 (init_mono): the interaction density is kappa
         adj_add(acc, 0, grp, F / (float)rg.kappa);
         adj_add(acc, 1, grp, F / (float)rg.kappa);
@@ -574,7 +615,7 @@ template <class R>
 __device__ __forceinline__ void adj_absorb(const Params<R>& P, const Pk<R>& pk, float* acc) {
     const int grp = P.adj_group[pk.layer];
     if (grp >= P.adj_ngroups) return;
-    adj_add(acc, 0, grp, (pk.ctot - pk.cpre) / (float)P.sc.region[pk.layer].mua);
+    adj_add(acc, 0, grp, (float)(pk.ctot - pk.cpre) / (float)P.sc.region[pk.layer].mua);
 }
 
 // Detector part of a retiring packet's contribution: sum of h_b over its bins.
@@ -620,7 +661,7 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
 template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ, bool MODS, bool BIG, bool VAR>
 __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers& B, Pk<R>& pk, Flight<R>& f,
                                                Stream<R, REPLAY>& rng, Cnt& c, int& act, unsigned long long* s_cnt,
-                                               double* s_mom, unsigned* s_bins, float* acc, uint2* vt) {
+                                               double* s_mom, unsigned* s_bins, float* acc, unsigned char* vt) {
     const auto& sc = scene_of<BIG>(P);
     const auto& sc64 = scene64_of<BIG>(P);
     using S = std::decay_t<decltype(sc)>;
@@ -630,13 +671,13 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // ---- adjoint: the end of a packet's first pass -- add its detector term to C
     // and trace the same packet again from its regenerated stream
     if (ADJ && act == A_DEATH && pk.phase == 0) {
-        pk.ctot += adj_detector_term(P, pk);
+        pk.ctot += (double)adj_detector_term(P, pk);
         rng.init(rng.seed, rng.inst, ((uint64_t)rng.p1 << 32) | rng.p0, nullptr, 0);
         emit(P, pk, rng);
         start_flight(f, rng);
         f.mode = S_LAUNCH;
         pk.phase = 1;
-        pk.cpre = 0.0f;
+        pk.cpre = 0.0;
         act = A_SWEEP;
     }
     // ---- retire a finished packet: detectors (kernelsMod.f90:302-306), counters
@@ -727,8 +768,8 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             }
             if (ADJ) {
                 pk.phase = 0;
-                pk.ctot = 0.0f;
-                pk.cpre = 0.0f;
+                pk.ctot = 0.0;
+                pk.cpre = 0.0;
             }
             emit(P, pk, rng);
             start_flight(f, rng);
@@ -749,9 +790,8 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             pk.weight = pk.weight - wa;
             // the interaction's voxel from the FP64 position (see start_step)
             const double ox = pk.pos.x + P.grid.xmax_d, oy = pk.pos.y + P.grid.ymax_d, oz = pk.pos.z + P.grid.zmax_d;
-            const int ci = (int)floor((double)P.grid.nx * ox / (2.0 * P.grid.xmax_d)) + 1;
-            const int cj = (int)floor((double)P.grid.ny * oy / (2.0 * P.grid.ymax_d)) + 1;
-            const int ck = (int)floor((double)P.grid.nz * oz / (2.0 * P.grid.zmax_d)) + 1;
+            int ci, cj, ck;
+            cell_of<R>(P.grid, ox, oy, oz, ci, cj, ck);
             if (ci < 1 || ci > P.grid.nx || cj < 1 || cj > P.grid.ny || ck < 1 || ck > P.grid.nz) {
                 pk.tflag = true;
                 act = A_DEATH;
@@ -1010,7 +1050,7 @@ struct Slots {
     // draw count of a Philox stream is 4 words a block less the words left
     uint32_t p0[kSlots], p1[kSlots], block[kSlots];
     uint32_t b0[kSlots], b1[kSlots], b2[kSlots], b3[kSlots];
-    float ctot[kA], cpre[kA];  // adjoint launches only
+    double ctot[kA], cpre[kA];  // adjoint launches only (FP64, see Pk)
 };
 // Regions addressable by the 8-bit layer field of a slot.
 constexpr int kMaxLayerField = 256;
@@ -1196,13 +1236,13 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     Pk<R> pk;
     pk.inst = 0;
     pk.phase = 0;
-    pk.ctot = pk.cpre = 0.0f;
+    pk.ctot = pk.cpre = 0.0;
     Flight<R> f;
     Stream<R, REPLAY> rng;
     Cnt c = {0, 0, 0, 0, 0, 0, 0};
     const unsigned long long t0 = global_ns();
     // this CTA's voxel-score tables (second-moment runs)
-    uint2* const vbase = VAR ? P.var_tab + (size_t)blockIdx.x * NS * kVarEntries : nullptr;
+    unsigned char* const vbase = VAR ? P.var_tab + (size_t)blockIdx.x * NS * kVarSlotBytes : nullptr;
     const unsigned lt = (1u << lane) - 1u;
     // ---- rounds: each round counting-sorts the live slots by action (warp
     // ballots and a per-warp scan, stable in slot order) and the warps take
@@ -1282,7 +1322,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
                 int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
                 transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
                     P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc,
-                    VAR ? vbase + (size_t)s * kVarEntries : nullptr);
+                    VAR ? vbase + (size_t)s * kVarSlotBytes : nullptr);
                 store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
             }
             int next = 0;

@@ -92,7 +92,7 @@ def test_adjoint_matches_crn_finite_differences():
     # the bounding medium is a 0.001 cm shell crossed in one step, so its mu_a and
     # mu_s move the loss by much less than one packet's contribution and the CRN
     # differences are exactly zero in every batch.  Compare where they vary.
-    informative = fd.std(axis=0) > 0
+    informative = np.abs(fd).max(axis=0) > 1e-9 * np.abs(fd).max()
     assert informative.sum() >= 12
     assert np.all(np.abs(z[informative]) < 3.0), (z, adj.mean(axis=0), fd.mean(axis=0))
 

@@ -24,7 +24,10 @@ def test_device_emitters_match_oracle(gpu, oracle, name):
     n = 4096
     gp, gd, gl = gpu.emit(flat, st, 100, n, 77, "fp64")
     op, od, ol = oracle.emit(flat, st, n, 77, "fp64", first=100)
-    assert np.array_equal(gp, op) and np.array_equal(gd, od) and np.array_equal(gl, ol)
+    # the same draws and formulas; sin/cos/atan2/log of CUDA and of the host C
+    # library may differ in the last bit
+    assert np.abs(gp - op).max() <= 1e-13 and np.abs(gd - od).max() <= 1e-13
+    assert np.array_equal(gl, ol)
     gp, gd, gl = gpu.emit(flat, st, 100, n, 77, "fp32")
     op, od, ol = oracle.emit(flat, st, n, 77, "fp32", first=100)
     assert np.abs(gp - op).max() <= 1e-5 * max(1.0, np.abs(op).max())

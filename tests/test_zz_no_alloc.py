@@ -67,3 +67,36 @@ def test_static_entry_point_rejects_bad_arguments(gpu):
     rc = lib.smcrt_run_device_static(flat.ptr(), C.byref(grid), C.byref(src), dets, 0, C.byref(opts), 0, 10, 1,
                                      None, None, None)
     assert rc == abi.ERR_ARG and b"fluence buffer" in lib.smcrt_last_error()
+
+
+def test_static_entry_point_leaves_device_memory_untouched(gpu):
+    """Callers whose device memory is owned by their own pool (or budgeted up front)
+    need the call to take no memory of its own: the device's free memory is the
+    same before and after an allocation-free run (after a first call, which only
+    looks up the static array's device address)."""
+    import torch
+    from signedmcrt_b200 import _lib
+    lib = _lib.lib()
+    st = P.benchmark_settings("box_slab")
+    flat = FlatScene(P.setup_simulation(st))
+    grid, src = st.grid_c(), st.source_c()
+    dets = (abi.Detector * 1)()
+    opts = abi.Options()
+    ncell = st.grid.nxg * st.grid.nyg * st.grid.nzg
+    jm = torch.zeros(ncell, dtype=torch.float64, device="cuda")
+
+    def call():
+        stats = abi.Stats()
+        rc = lib.smcrt_run_device_static(flat.ptr(), C.byref(grid), C.byref(src), dets, 0, C.byref(opts), 0, 20000,
+                                         5, C.c_void_p(jm.data_ptr()), None, C.byref(stats))
+        assert rc == abi.OK, lib.smcrt_last_error().decode()
+        return stats.to_dict()
+
+    call()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    st1 = call()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert st1["packets"] == 20000
+    assert free1 == free0, (free0, free1)
