@@ -180,7 +180,7 @@ typedef struct smcrt_options {
     int32_t end_early;     /* test kernel: kill after the 4th scatter (test_scat.f90:65) */
     int32_t block_size;    /* threads per CTA: 0 or 640 (a CTA holds 1280 FP32 / 640 FP64 packets) */
     int32_t blocks_per_sm; /* 0 = library default (persistent grid = SMs * this) */
-    int32_t max_trace_steps; /* per tauint2 sphere-trace step cap; 0 = 1,000,000 */
+    int32_t max_trace_steps; /* per tauint2 sphere-trace step cap; 0 = 1,000,000; at most 2,097,151 */
     double eps;            /* surface epsilon; <= 0 selects the reference's 1e-8
                               (inttau2.f90:44) in both precisions (FP32 transport
                               takes every decision against it in FP64) */

@@ -209,6 +209,15 @@ double near_band(double eps, const smcrt_grid& g) {
     return std::fmax(2.0 * eps, 16.0 * ulp);
 }
 
+// The per-flight sphere-trace step count shares its slot word with the
+// nearest-region cache: 21 bits.
+constexpr int kMaxTraceSteps = (1 << 21) - 1;
+int check_steps(const smcrt_options* o) {
+    if (o && o->max_trace_steps > kMaxTraceSteps)
+        return fail(SMCRT_ERR_ARG, "options: max_trace_steps must be at most " + std::to_string(kMaxTraceSteps));
+    return SMCRT_OK;
+}
+
 int pick_device(int& dev, int& nsm) {
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
@@ -344,6 +353,7 @@ void fill_params(Params<R>* P, const smcrt_scene* scene, const smcrt_grid* grid,
     const int prec = (sizeof(R) == 4) ? SMCRT_FP32 : SMCRT_FP64;
     P->eps = (R)((o && o->eps > 0) ? o->eps : default_eps(prec, *grid));
     P->near_band = (R)near_band((double)P->eps, *grid);
+    P->cache_ok = cache_policy(scene, grid, (int)sizeof(R), &P->cache_margin) ? 1 : 0;
     P->normal_h = (o && o->normal_h > 0) ? o->normal_h : 1e-6;
     P->instance = o ? o->instance : 0u;
     P->tcopies = 1;
@@ -605,6 +615,7 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
     const int kern = opts ? opts->kernel : SMCRT_KERNEL_PATHLENGTH;
     if (prec != SMCRT_FP32 && prec != SMCRT_FP64) return fail(SMCRT_ERR_ARG, "options: unknown precision");
     if (kern < SMCRT_KERNEL_PATHLENGTH || kern > SMCRT_KERNEL_TEST) return fail(SMCRT_ERR_ARG, "options: unknown kernel");
+    if (check_steps(opts)) return SMCRT_ERR_ARG;
     DetT dtab[kMaxDetectors];
     long long nbins = 0;
     rc = fill_dets(dtab, dets, ndet, scene->nregions, nbins);
@@ -1206,6 +1217,7 @@ int32_t smcrt_batch_create(const smcrt_scene* scene, const smcrt_grid* grid, con
         return fail(SMCRT_ERR_ARG, "batch: pathlength and weight kernels only");
     if (opts && opts->block_size > 0 && opts->block_size != kBlock)
         return fail(SMCRT_ERR_ARG, "options: block_size must be 0 or " + std::to_string(kBlock));
+    if (check_steps(opts)) return SMCRT_ERR_ARG;
     DetT dtab[kMaxDetectors];
     long long nbins = 0;
     rc = fill_dets(dtab, dets, ndet, scene->nregions, nbins);
@@ -1630,6 +1642,7 @@ int32_t smcrt_run_device_static(const smcrt_scene* scene, const smcrt_grid* grid
     if (opts && opts->kernel != SMCRT_KERNEL_PATHLENGTH && opts->kernel != SMCRT_KERNEL_WEIGHT &&
         opts->kernel != SMCRT_KERNEL_TEST)
         return fail(SMCRT_ERR_ARG, "options: unknown kernel");
+    if (check_steps(opts)) return SMCRT_ERR_ARG;
     const int prec = opts ? opts->precision : SMCRT_FP32;
     if (prec == SMCRT_FP64)
         return run_static_t<double>(scene, grid, source, dets, ndet, opts, first, count, seed, jmean_dev, det_bins_dev,

@@ -536,6 +536,10 @@ struct Params {
     int max_steps;
     R eps;
     R near_band;  // FP32 transport: sweeps closer than this to a surface are taken in FP64
+    // nearest-region cache: allowed (every region 1-Lipschitz) and the rounding
+    // margin of its test (FP32 transport: the FP32 sweeps' margin for both sweeps)
+    int cache_ok;
+    double cache_margin;
     double normal_h;
     unsigned long long seed;
     unsigned long long budget_ns;  // per-launch device time budget (0 = none)

@@ -50,6 +50,11 @@ cudaError_t launch_render(int precision, const smcrt_scene* scene, const int sam
 // cull margin.
 template <class R>
 void fill_scene(SceneT<R>& d, const smcrt_scene* s);
+bool region_bound(const smcrt_scene* s, int r, double c[3], double* rad);
+// Whether every region's SDF is an exact Euclidean distance under a rigid
+// transform (the nearest-region cache needs 1-Lipschitz regions), and the
+// margin covering the rounding of its test in precision `bytes` (4 or 8).
+bool cache_policy(const smcrt_scene* s, const smcrt_grid* grid, int bytes, double* margin);
 template <class R>
 void scene_tables(const smcrt_scene* s, const smcrt_grid* grid, std::vector<DPrim<R>>& prims,
                   std::vector<DRegion<R>>& regions, std::vector<R>& bounds, R* margin);

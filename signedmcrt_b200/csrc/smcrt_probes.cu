@@ -101,6 +101,25 @@ bool region_bound(const smcrt_scene* s, int r, double c[3], double* rad) {
     return std::isfinite(c[0]) && std::isfinite(c[1]) && std::isfinite(c[2]);
 }
 
+bool cache_policy(const smcrt_scene* s, const smcrt_grid* grid, int bytes, double* margin) {
+    double scale = 1.0;
+    if (grid) scale = std::fmax(scale, std::fmax(grid->xmax, std::fmax(grid->ymax, grid->zmax)));
+    for (int i = 0; i < s->nregions; ++i) {
+        double c[3], rad;
+        if (!region_bound(s, i, c, &rad)) {
+            *margin = 0;
+            return false;
+        }
+        scale = std::fmax(scale, std::fabs(c[0]) + std::fabs(c[1]) + std::fabs(c[2]) + rad);
+    }
+    // 64 ulps of the coordinates' magnitude: the transform and the primitive's
+    // few operations round a region's value by a handful of ulps
+    int e;
+    std::frexp(scale, &e);
+    *margin = std::ldexp(64.0, e - (bytes == 4 ? 24 : 53));
+    return true;
+}
+
 template <class R>
 void scene_tables(const smcrt_scene* s, const smcrt_grid* grid, std::vector<DPrim<R>>& prims,
                   std::vector<DRegion<R>>& regions, std::vector<R>& bounds, R* margin) {

@@ -284,12 +284,25 @@ enum Act : int { A_NEW = 0, A_SWEEP, A_WALK, A_CROSS, A_INTERACT, A_DEATH, A_DON
 // What the next sweep is for.
 enum SweepMode : int { S_LAUNCH = 0, S_TOP, S_STEP, S_CROSS };
 
+// FP32 bounds of a length: rounded down (a clearance) or up (a distance moved).
+__device__ __forceinline__ float float_rd(float x) { return x; }
+__device__ __forceinline__ float float_rd(double x) { return __double2float_rd(x); }
+__device__ __forceinline__ float float_ru(float x) { return x; }
+__device__ __forceinline__ float float_ru(double x) { return __double2float_ru(x); }
+
 template <class R>
 struct Flight {
     R tau, taurun, dsdf;  // optical depth to spend / spent; current step length
     int steps;            // sphere-tracing steps of the current inner loop
     int mode;             // SweepMode of the next sweep
     bool last;            // the current step spends the remaining optical depth
+    // Nearest-region cache (see nearest_cached): valid flag, the nearest region
+    // at the last full sweep, whether another region contained the point there,
+    // and the clearance -- a lower bound on every other region's |d| less the
+    // path travelled since that sweep.
+    bool cache, negx;
+    int nk;
+    float clear;
     // Integer voxel walk of the current step (update_grids, inttau2.f90:213-292):
     // parametric distance to the next x/y/z face, distance walked, and the cell.
     // During a crossing the same storage holds the position before the step.
@@ -308,11 +321,16 @@ struct Flight {
 // All regions at one point (the sweep of tauint2, inttau2.f90:51-55,86-96,104-108):
 // signed minimum, minimum |d|, region 0's value, region L's value, the first
 // region containing the point (and its value), and the launch layer
-// (kernelsMod.f90:275-280: innermost containing region).
+// (kernelsMod.f90:275-280: innermost containing region).  For the nearest-region
+// cache also: the region of the minimum |d| (k), a lower bound on every other
+// region's |d| (m2), and whether another region contains the point (negx).
 template <class T>
 struct SweepOut {
     T mn, mna, d0, dsL, dsN;
     int nl, lay;
+    T m2;
+    int k;
+    bool negx;
 };
 //
 // Device-memory scenes (SceneG) skip regions by their bounding spheres.  A
@@ -325,32 +343,49 @@ struct SweepOut {
 // there).  Regions 0 and L are always evaluated (their values are outputs).
 template <class T, bool MODS = true, class S = SceneT<T>>
 __device__ __forceinline__ SweepOut<T> sweep_regions(const S& sc, V3<T> p, int L) {
-    SweepOut<T> o{(T)INFINITY, (T)INFINITY, (T)0, (T)0, (T)0, -1, 0};
+    SweepOut<T> o{(T)INFINITY, (T)INFINITY, (T)0, (T)0, (T)0, -1, 0, (T)INFINITY, 0, false};
     T inner = (T)INFINITY;
+    int nneg = 0;
+    bool kneg = false;
     for (int i = 0; i < sc.nregions; ++i) {
         if constexpr (!std::is_same<S, SceneT<T>>::value) {
             const T br = sc.bound[4 * i + 3];
             if (br >= (T)0 && i != 0 && i != L && o.mna < (T)INFINITY) {
                 const T dx = p.x - sc.bound[4 * i], dy = p.y - sc.bound[4 * i + 1], dz = p.z - sc.bound[4 * i + 2];
+                const T r2 = dx * dx + dy * dy + dz * dz;
                 const T lim = o.mna + sc.cull_margin + br;
-                if (dx * dx + dy * dy + dz * dz > lim * lim) continue;
+                if (r2 > lim * lim) {
+                    // outside its bounding sphere: |d| >= distance to the sphere
+                    o.m2 = fmin(o.m2, sqrt(r2) - br);
+                    continue;
+                }
             }
         }
         const T d = eval_region<T, MODS, S>(sc, i, p);
+        const T a = fabs(d);
         o.mn = fmin(o.mn, d);
-        o.mna = fmin(o.mna, fabs(d));
+        if (a < o.mna) {
+            o.m2 = o.mna;
+            o.mna = a;
+            o.k = i;
+            kneg = d < (T)0;
+        } else {
+            o.m2 = fmin(o.m2, a);
+        }
+        nneg += d < (T)0;
         if (i == 0) o.d0 = d;
         if (i == L) o.dsL = d;
         if (o.nl < 0 && d < (T)0) {
             o.nl = i;
             o.dsN = d;
         }
-        const T a = (d > (T)0) ? (T)999.0 : fabs(d);
-        if (a < inner) {
-            inner = a;
+        const T ai = (d > (T)0) ? (T)999.0 : a;
+        if (ai < inner) {
+            inner = ai;
             o.lay = i;
         }
     }
+    o.negx = nneg - (int)kneg > 0;
     return o;
 }
 
@@ -646,6 +681,7 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
     if (a < 0) {
         if (ADJ) adj_track(P, pk, acc, (float)f.dsdf, 0.0f);  // a step outside the grid
         pk.pos = advance(pk.pos, f.dsdf, pk.dir);
+        f.clear = __fsub_rd(f.clear, float_ru(f.dsdf));
         if (f.last) return end_flight(P, pk);
         f.mode = S_STEP;
         return A_SWEEP;
@@ -851,17 +887,47 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // to ~1e-7 cm, ten times eps, and that noise changed how many refracted packets
     // the eps rule kills (-0.8% fluence).  Such sweeps are deferred as A_PRECISE so
     // that they run together, not one lane per warp.
+    //
+    // Nearest-region cache.  A full sweep records its nearest region k, a lower
+    // bound m2 on every other region's |d|, and whether another region contains
+    // the point; every move subtracts its length from the bound (regions are
+    // 1-Lipschitz: exact distances under rigid transforms, checked on the host).
+    // While |d_k| plus a rounding margin stays below that clearance, no other
+    // region can be nearer or have changed sign, so region k alone gives the
+    // sweep's outputs that a tracing step uses (min |d| and the sign of the
+    // signed minimum) -- the same values as the full sweep.  Boundary events
+    // (crossing sweeps, launches) always sweep in full; the counters still count
+    // the reference's evaluations of every region.
     if (act == A_SWEEP || act == A_PRECISE) {
         const int L = pk.layer;
-        SweepOut<R> sw;
-        bool precise = false, defer = false;
-        if (sizeof(R) == 4 && act == A_PRECISE) {
-            const SweepOut<double> s64 = sweep_regions<double, MODS, S64>(sc64, pk.pos, L);
-            sw = SweepOut<R>{(R)s64.mn, (R)s64.mna, (R)s64.d0, (R)s64.dsL, (R)s64.dsN, s64.nl, s64.lay};
-            precise = true;
-        } else {
-            sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L);
-            defer = sizeof(R) == 4 && (sw.mna <= P.near_band || f.mode == S_CROSS);
+        SweepOut<R> sw{};
+        bool precise = false, defer = false, full = true;
+        const bool want64 = sizeof(R) == 4 && act == A_PRECISE;
+        if (!ADJ && f.cache && (f.mode == S_STEP || f.mode == S_TOP)) {
+            const double dk = want64 ? eval_region<double, MODS, S64>(sc64, f.nk, pk.pos)
+                                     : (double)eval_region<R, MODS, S>(sc, f.nk, cv<R>(pk.pos));
+            if (fabs(dk) + P.cache_margin < (double)f.clear) {
+                full = false;
+                sw.mna = (R)fabs(dk);
+                sw.mn = (dk < 0.0 || f.negx) ? (R)-1 : sw.mna;
+                precise = want64;
+                defer = sizeof(R) == 4 && !want64 && sw.mna <= P.near_band;
+            }
+        }
+        if (full) {
+            if (want64) {
+                const SweepOut<double> s64 = sweep_regions<double, MODS, S64>(sc64, pk.pos, L);
+                sw = SweepOut<R>{(R)s64.mn, (R)s64.mna, (R)s64.d0, (R)s64.dsL, (R)s64.dsN, s64.nl, s64.lay,
+                                 (R)s64.m2, s64.k, s64.negx};
+                precise = true;
+            } else {
+                sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L);
+                defer = sizeof(R) == 4 && (sw.mna <= P.near_band || f.mode == S_CROSS);
+            }
+            f.cache = !ADJ && P.cache_ok && f.mode != S_CROSS;
+            f.nk = sw.k;
+            f.negx = sw.negx;
+            f.clear = float_rd(sw.m2);
         }
         if (defer) {
             act = A_PRECISE;
@@ -994,6 +1060,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
         if (walk_segment<R, BATCH, ADJ, VAR>(P, pk, f, c, acc, vt)) {
             pk.pos = advance(pk.pos, f.dsdf, pk.dir);
+            f.clear = __fsub_rd(f.clear, float_ru(f.dsdf));
             if (f.last) {
                 act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
             } else {
@@ -1029,6 +1096,17 @@ struct SlotCount {
 #define SMCRT_GROUP_ORDER 0x05431214u
 #endif
 constexpr int kGroups = 5;
+// Drain mode: at most this many live slots in a CTA (a few per warp), each run
+// for kDrainPasses passes per round.
+#ifndef SMCRT_DRAIN_LIVE_PER_WARP
+#define SMCRT_DRAIN_LIVE_PER_WARP 4
+#endif
+#ifndef SMCRT_DRAIN_PASSES
+#define SMCRT_DRAIN_PASSES 16
+#endif
+constexpr int kDrainLive = SMCRT_DRAIN_LIVE_PER_WARP * (kBlock / 32);
+constexpr int kDrainPasses = SMCRT_DRAIN_PASSES;
+static_assert(SMCRT_DRAIN_LIVE_PER_WARP <= 32, "one drain item per lane at most");
 __device__ __forceinline__ int act_group(int act) { return (int)((SMCRT_GROUP_ORDER >> (4 * act)) & 0xFu); }
 template <class R, bool ADJ, int kSlots = SlotCount<R>::n>
 struct Slots {
@@ -1044,7 +1122,10 @@ struct Slots {
     // act | mode << 3 | last << 5 | tflag << 6 | adjoint pass << 7 | layer << 8 |
     // pk.flags << 16 | rng.flags << 24
     uint32_t meta[kSlots];
-    int steps[kSlots], nscatt[kSlots];
+    // trace steps | nearest region << 21 | negx << 29 | cache valid << 30
+    uint32_t steps[kSlots];
+    int nscatt[kSlots];
+    float clr[ADJ ? 1 : kSlots];  // nearest-region cache clearance (not in adjoint launches)
     uint32_t bl[kSlots];  // bounces (<= 1001) | rng.left << 11 | batch instance << 14
     // Philox block counter (replay builds: the injected uniforms consumed); the
     // draw count of a Philox stream is 4 words a block less the words left
@@ -1090,7 +1171,12 @@ __device__ __forceinline__ int load_slot(const Slots<R, ADJ>& sl, int s, const P
     pk.weight = sl.w[s];
     f.tau = sl.tau[s];
     f.taurun = sl.taurun[s];
-    f.steps = sl.steps[s];
+    const uint32_t sw = sl.steps[s];
+    f.steps = (int)(sw & 0x1FFFFFu);
+    f.nk = (int)((sw >> 21) & 255u);
+    f.negx = (sw >> 29) & 1u;
+    f.cache = !ADJ && ((sw >> 30) & 1u);
+    f.clear = ADJ ? 0.0f : sl.clr[ADJ ? 0 : s];
     pk.nscatt = sl.nscatt[s];
     const uint32_t bl = sl.bl[s];
     pk.bounces = (int)(bl & 0x7FFu);
@@ -1157,7 +1243,9 @@ __device__ __forceinline__ void store_slot(Slots<R, ADJ>& sl, int s, int act, co
     sl.w[s] = pk.weight;
     sl.tau[s] = f.tau;
     sl.taurun[s] = f.taurun;
-    sl.steps[s] = f.steps;
+    sl.steps[s] = (uint32_t)f.steps | ((uint32_t)f.nk << 21) | ((uint32_t)f.negx << 29) |
+                  ((uint32_t)(!ADJ && f.cache) << 30);
+    if (!ADJ) sl.clr[ADJ ? 0 : s] = f.clear;
     sl.nscatt[s] = pk.nscatt;
     sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 11) | ((uint32_t)(BATCH ? pk.inst : 0) << 14);
     sl.p0[s] = rng.p0;
@@ -1314,17 +1402,30 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         const int stop = s_stop;
         __syncthreads();
         if (total == 0 || stop) break;
-        const int nchunks = (total + 31) >> 5;
+        // drain: few live packets left in this CTA (the end of a launch, or long
+        // histories such as a packet creeping along a wall in steps of its
+        // distance to it).  They are spread one to a few per warp (item
+        // warp + NW x lane) and each runs kDrainPasses passes before it goes back
+        // to its slot, so that a long chain of dependent steps does not wait for
+        // a sort per step.  Otherwise warps take 32-item chunks.  One call site
+        // of the pass serves both.
+        const bool drain = total <= kDrainLive;
+        const int nchunks = drain ? NW : (total + 31) >> 5;
+        const int reps = drain ? kDrainPasses : 1;
         for (int chunk = warp; chunk < nchunks;) {
-            const int i = chunk * 32 + (int)lane;
+            const int i = drain ? chunk + NW * (int)lane : chunk * 32 + (int)lane;
             if (i < total) {
                 const int s = s_list[i];
                 int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-                transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
-                    P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc,
-                    VAR ? vbase + (size_t)s * kVarSlotBytes : nullptr);
+                for (int r = 0; r < reps; ++r) {
+                    transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
+                        P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc,
+                        VAR ? vbase + (size_t)s * kVarSlotBytes : nullptr);
+                    if (act == A_DONE) break;
+                }
                 store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
             }
+            if (drain) break;
             int next = 0;
             if (lane == 0) next = atomicAdd(&s_next, 1);
             chunk = __shfl_sync(0xffffffffu, next, 0);

@@ -114,3 +114,14 @@ def test_render_checks_its_arguments_before_the_device():
         with pytest.raises(_lib.SmcrtError) as e:
             T.render(arr, (4, 4, 4), (1.0, 1.0, 1.0))
         assert e.value.code == abi.ERR_NO_DEVICE
+
+
+def test_trace_step_cap_is_bounded_before_the_device():
+    """The per-flight step count shares its slot word with the nearest-region
+    cache (21 bits): a larger max_trace_steps is refused with SMCRT_ERR_ARG
+    before any device is touched."""
+    from signedmcrt_b200 import _lib, presets as P, transport as T
+    st = P.benchmark_settings("box_slab")
+    with pytest.raises(_lib.SmcrtError) as e:
+        T.Transport(P.setup_simulation(st), st, max_trace_steps=(1 << 21))
+    assert e.value.code == abi.ERR_ARG

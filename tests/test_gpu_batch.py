@@ -98,3 +98,8 @@ def test_fp32_error_matches_fp64_error():
     from signedmcrt_b200.accuracy import error_table
     t = error_table("box_slab", 200000)
     assert 0.85 < t["ratio"] < 1.15, t
+    # per voxel, with standard errors from the second moments
+    assert t["variance_overflows"] == 0, t
+    for tag in ("fp32", "fp64"):
+        assert t["chi2_" + tag]["voxels"] > 1000 and t["chi2_" + tag]["chi2_per_voxel"] < 1.15, t
+        assert t["chi2_" + tag]["frac_z_gt_4"] < 2e-3, t
