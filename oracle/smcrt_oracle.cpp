@@ -647,6 +647,7 @@ template <class R>
 struct SweepRes {
     R mn, mna;
     int nl, lay;
+    bool f64;  // taken in FP64
 };
 template <class T>
 void sweep_stats(const T* v, int N, T& mn, T& mna, int& nl, int& lay) {
@@ -671,12 +672,14 @@ SweepRes<R> sweep(const Scene<R>& sc, const Scene<double>& sc64, const Pol& pol,
                   R* out) {
     const int N = (int)sc.regions.size();
     SweepRes<R> o;
+    o.f64 = sizeof(R) == 8;
     if (!(pol.near_f64 && force64)) {
         const V3<R> p = cv<R>(pos);
         for (int i = 0; i < N; ++i) out[i] = eval_region(sc, i, p);
         sweep_stats(out, N, o.mn, o.mna, o.nl, o.lay);
         if (!pol.near_f64 || sizeof(R) == 8 || o.mna > (R)pol.near_band) return o;
     }
+    o.f64 = true;
     thread_local std::vector<double> v64;
     v64.resize(N);
     for (int i = 0; i < N; ++i) v64[i] = eval_region(sc64, i, pos);
@@ -735,8 +738,13 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
     for (;;) {
         // dstmp holds the values of the latest sweep: at a surface they are the
         // reference's dstmp sweep (:104-108), taken at the same point
-        R dsdf = sweep(sc, sc64, pol, pos, false, dstmp.data()).mna;
+        const SweepRes<R> top = sweep(sc, sc64, pol, pos, false, dstmp.data());
+        R dsdf = top.mna;
         c.sdf += N;
+        // device FP32 semantics: an FP64 sweep that finds the surface within half
+        // of near_band sends the next step's sweep straight to FP64 (a move of
+        // min|d| changes every |d| by at most that, so it is within near_band)
+        bool near = pol.near_f64 && top.f64 && (R)2 * top.mna <= (R)pol.near_band;
         // reference: kill if d < eps (inttau2.f90:58); device semantics also kills
         // at d == eps, where the trace loop (d > eps, :63) has already stopped
         if (pol.kill_le ? dsdf <= eps : dsdf < eps) {
@@ -767,9 +775,10 @@ void tauint2(const Scene<R>& sc, const Scene<double>& sc64, const GridD& g, cons
                 break;
             }
             if (!ok) break;
-            const SweepRes<R> sw = sweep(sc, sc64, pol, pos, false, dstmp.data());
+            const SweepRes<R> sw = sweep(sc, sc64, pol, pos, near, dstmp.data());
             c.sdf += N;
             dsdf = sw.mna;
+            near = pol.near_f64 && sw.f64 && (R)2 * sw.mna <= (R)pol.near_band;
             if (sw.mn >= (R)0) {
                 pk.tflag = true;
                 break;

@@ -276,6 +276,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #ifndef SMCRT_WALK_SEGMENTS
 #define SMCRT_WALK_SEGMENTS 3
 #endif
+// FP64 near-surface steps chained within one pass (FP32 transport)
+#ifndef SMCRT_PRECISE_CHAIN
+#define SMCRT_PRECISE_CHAIN 8
+#endif
+constexpr int kPreciseChain = SMCRT_PRECISE_CHAIN;
 
 // Per-lane actions of the flattened transport loop.
 // A_PRECISE (FP32 transport): a sweep within the FP64 band of a surface, or resolving a
@@ -303,6 +308,10 @@ struct Flight {
     bool cache, negx;
     int nk;
     float clear;
+    // FP32 transport: the last sweep was taken in FP64 and found the surface
+    // within half of near_band, so the next step's sweep is within near_band too
+    // (a move of min|d| changes every |d| by at most that) and goes straight to FP64
+    bool near;
     // Integer voxel walk of the current step (update_grids, inttau2.f90:213-292):
     // parametric distance to the next x/y/z face, distance walked, and the cell.
     // During a crossing the same storage holds the position before the step.
@@ -898,6 +907,11 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // signed minimum) -- the same values as the full sweep.  Boundary events
     // (crossing sweeps, launches) always sweep in full; the counters still count
     // the reference's evaluations of every region.
+    // A run of FP64 near-surface steps (f.near) continues in this pass, up to
+    // kPreciseChain steps: the warp is already on FP64 sweeps, and each step
+    // would otherwise cost a round.
+    bool did64 = false;
+    for (int chain = 0;; ++chain) {
     if (act == A_SWEEP || act == A_PRECISE) {
         const int L = pk.layer;
         SweepOut<R> sw{};
@@ -930,6 +944,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             f.clear = float_rd(sw.m2);
         }
         if (defer) {
+            f.near = false;
             act = A_PRECISE;
         } else {
             act = A_SWEEP;
@@ -940,6 +955,8 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             c.sdf += N;
             f.dsdf = mna;
             const int mode = f.mode;
+            f.near = sizeof(R) == 4 && precise && mode != S_CROSS && (R)2 * mna <= P.near_band;
+            did64 = did64 || precise;
             if (mode == S_LAUNCH || mode == S_TOP) {
                 // top of tauint2's outer loop (:51-61).  At launch the same sweep also
                 // gives the layer (the reference evaluates the same point twice).
@@ -1065,9 +1082,11 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
             } else {
                 f.mode = S_STEP;
-                act = A_SWEEP;
+                act = (sizeof(R) == 4 && f.near) ? A_PRECISE : A_SWEEP;
             }
         }
+    }
+    if (!(did64 && act == A_PRECISE && f.near && chain < kPreciseChain)) break;
     }
 }
 
@@ -1122,7 +1141,7 @@ struct Slots {
     // act | mode << 3 | last << 5 | tflag << 6 | adjoint pass << 7 | layer << 8 |
     // pk.flags << 16 | rng.flags << 24
     uint32_t meta[kSlots];
-    // trace steps | nearest region << 21 | negx << 29 | cache valid << 30
+    // trace steps | nearest region << 21 | negx << 29 | cache valid << 30 | near << 31
     uint32_t steps[kSlots];
     int nscatt[kSlots];
     float clr[ADJ ? 1 : kSlots];  // nearest-region cache clearance (not in adjoint launches)
@@ -1176,6 +1195,7 @@ __device__ __forceinline__ int load_slot(const Slots<R, ADJ>& sl, int s, const P
     f.nk = (int)((sw >> 21) & 255u);
     f.negx = (sw >> 29) & 1u;
     f.cache = !ADJ && ((sw >> 30) & 1u);
+    f.near = (sw >> 31) & 1u;
     f.clear = ADJ ? 0.0f : sl.clr[ADJ ? 0 : s];
     pk.nscatt = sl.nscatt[s];
     const uint32_t bl = sl.bl[s];
@@ -1244,7 +1264,7 @@ __device__ __forceinline__ void store_slot(Slots<R, ADJ>& sl, int s, int act, co
     sl.tau[s] = f.tau;
     sl.taurun[s] = f.taurun;
     sl.steps[s] = (uint32_t)f.steps | ((uint32_t)f.nk << 21) | ((uint32_t)f.negx << 29) |
-                  ((uint32_t)(!ADJ && f.cache) << 30);
+                  ((uint32_t)(!ADJ && f.cache) << 30) | ((uint32_t)f.near << 31);
     if (!ADJ) sl.clr[ADJ ? 0 : s] = f.clear;
     sl.nscatt[s] = pk.nscatt;
     sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 11) | ((uint32_t)(BATCH ? pk.inst : 0) << 14);
