@@ -276,11 +276,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #ifndef SMCRT_WALK_SEGMENTS
 #define SMCRT_WALK_SEGMENTS 3
 #endif
-// FP64 near-surface steps chained within one pass (FP32 transport)
-#ifndef SMCRT_PRECISE_CHAIN
-#define SMCRT_PRECISE_CHAIN 8
+// The nearest-region cache (1: built in; 0: every sweep evaluates every region)
+#ifndef SMCRT_NEAREST_CACHE
+#define SMCRT_NEAREST_CACHE 1
 #endif
-constexpr int kPreciseChain = SMCRT_PRECISE_CHAIN;
+constexpr bool kNearestCache = SMCRT_NEAREST_CACHE != 0;
 
 // Per-lane actions of the flattened transport loop.
 // A_PRECISE (FP32 transport): a sweep within the FP64 band of a surface, or resolving a
@@ -907,17 +907,12 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // signed minimum) -- the same values as the full sweep.  Boundary events
     // (crossing sweeps, launches) always sweep in full; the counters still count
     // the reference's evaluations of every region.
-    // A run of FP64 near-surface steps (f.near) continues in this pass, up to
-    // kPreciseChain steps: the warp is already on FP64 sweeps, and each step
-    // would otherwise cost a round.
-    bool did64 = false;
-    for (int chain = 0;; ++chain) {
     if (act == A_SWEEP || act == A_PRECISE) {
         const int L = pk.layer;
         SweepOut<R> sw{};
         bool precise = false, defer = false, full = true;
         const bool want64 = sizeof(R) == 4 && act == A_PRECISE;
-        if (!ADJ && f.cache && (f.mode == S_STEP || f.mode == S_TOP)) {
+        if (kNearestCache && !ADJ && f.cache && (f.mode == S_STEP || f.mode == S_TOP)) {
             const double dk = want64 ? eval_region<double, MODS, S64>(sc64, f.nk, pk.pos)
                                      : (double)eval_region<R, MODS, S>(sc, f.nk, cv<R>(pk.pos));
             if (fabs(dk) + P.cache_margin < (double)f.clear) {
@@ -938,7 +933,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L);
                 defer = sizeof(R) == 4 && (sw.mna <= P.near_band || f.mode == S_CROSS);
             }
-            f.cache = !ADJ && P.cache_ok && f.mode != S_CROSS;
+            f.cache = kNearestCache && !ADJ && P.cache_ok && f.mode != S_CROSS;
             f.nk = sw.k;
             f.negx = sw.negx;
             f.clear = float_rd(sw.m2);
@@ -956,7 +951,6 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             f.dsdf = mna;
             const int mode = f.mode;
             f.near = sizeof(R) == 4 && precise && mode != S_CROSS && (R)2 * mna <= P.near_band;
-            did64 = did64 || precise;
             if (mode == S_LAUNCH || mode == S_TOP) {
                 // top of tauint2's outer loop (:51-61).  At launch the same sweep also
                 // gives the layer (the reference evaluates the same point twice).
@@ -1085,8 +1079,6 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 act = (sizeof(R) == 4 && f.near) ? A_PRECISE : A_SWEEP;
             }
         }
-    }
-    if (!(did64 && act == A_PRECISE && f.near && chain < kPreciseChain)) break;
     }
 }
 
