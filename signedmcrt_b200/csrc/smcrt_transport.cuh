@@ -281,6 +281,12 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define SMCRT_NEAREST_CACHE 1
 #endif
 constexpr bool kNearestCache = SMCRT_NEAREST_CACHE != 0;
+// FP32 transport: extra passes a packet may take within one round while it is on a
+// run of FP64 near-surface steps (0: none; each step waits for the next round)
+#ifndef SMCRT_PRECISE_CHAIN
+#define SMCRT_PRECISE_CHAIN 0
+#endif
+constexpr int kPreciseChain = SMCRT_PRECISE_CHAIN;
 
 // Per-lane actions of the flattened transport loop.
 // A_PRECISE (FP32 transport): a sweep within the FP64 band of a surface, or resolving a
@@ -350,13 +356,19 @@ struct SweepOut {
 // and larger than that minimum, so it changes none of the outputs (the signed
 // minimum only matters through its sign, and the region contains no point
 // there).  Regions 0 and L are always evaluated (their values are outputs).
+//
+// only >= 0: the nearest-region cache holds, so only region `only` is evaluated
+// (mn, mna and k then describe that region alone; the caller supplies the sign
+// of the other regions).  Lanes of one warp that sweep in full and lanes that
+// sweep one region share this loop, so a warp evaluates each region at most once.
 template <class T, bool MODS = true, class S = SceneT<T>>
-__device__ __forceinline__ SweepOut<T> sweep_regions(const S& sc, V3<T> p, int L) {
+__device__ __forceinline__ SweepOut<T> sweep_regions(const S& sc, V3<T> p, int L, int only = -1) {
     SweepOut<T> o{(T)INFINITY, (T)INFINITY, (T)0, (T)0, (T)0, -1, 0, (T)INFINITY, 0, false};
     T inner = (T)INFINITY;
     int nneg = 0;
     bool kneg = false;
     for (int i = 0; i < sc.nregions; ++i) {
+        if (only >= 0 && i != only) continue;
         if constexpr (!std::is_same<S, SceneT<T>>::value) {
             const T br = sc.bound[4 * i + 3];
             if (br >= (T)0 && i != 0 && i != L && o.mna < (T)INFINITY) {
@@ -910,29 +922,26 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     if (act == A_SWEEP || act == A_PRECISE) {
         const int L = pk.layer;
         SweepOut<R> sw{};
-        bool precise = false, defer = false, full = true;
-        const bool want64 = sizeof(R) == 4 && act == A_PRECISE;
-        if (kNearestCache && !ADJ && f.cache && (f.mode == S_STEP || f.mode == S_TOP)) {
-            const double dk = want64 ? eval_region<double, MODS, S64>(sc64, f.nk, pk.pos)
-                                     : (double)eval_region<R, MODS, S>(sc, f.nk, cv<R>(pk.pos));
-            if (fabs(dk) + P.cache_margin < (double)f.clear) {
-                full = false;
-                sw.mna = (R)fabs(dk);
-                sw.mn = (dk < 0.0 || f.negx) ? (R)-1 : sw.mna;
-                precise = want64;
-                defer = sizeof(R) == 4 && !want64 && sw.mna <= P.near_band;
-            }
+        bool precise = false, defer = false;
+        // the cache holds for a tracing step when |d_k| + margin stays below the
+        // clearance: |d_k| was the step length f.dsdf before the move, so it is
+        // at most 2 f.dsdf now (the move is already off the clearance)
+        const bool cached = kNearestCache && !ADJ && f.cache && f.mode == S_STEP &&
+                            (double)(2 * f.dsdf) + P.cache_margin < (double)f.clear;
+        const int only = cached ? f.nk : -1;
+        if (sizeof(R) == 4 && act == A_PRECISE) {
+            const SweepOut<double> s64 = sweep_regions<double, MODS, S64>(sc64, pk.pos, L, only);
+            sw = SweepOut<R>{(R)s64.mn, (R)s64.mna, (R)s64.d0, (R)s64.dsL, (R)s64.dsN, s64.nl, s64.lay,
+                             (R)s64.m2, s64.k, s64.negx};
+            precise = true;
+        } else {
+            sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L, only);
+            defer = sizeof(R) == 4 && (sw.mna <= P.near_band || f.mode == S_CROSS);
         }
-        if (full) {
-            if (want64) {
-                const SweepOut<double> s64 = sweep_regions<double, MODS, S64>(sc64, pk.pos, L);
-                sw = SweepOut<R>{(R)s64.mn, (R)s64.mna, (R)s64.d0, (R)s64.dsL, (R)s64.dsN, s64.nl, s64.lay,
-                                 (R)s64.m2, s64.k, s64.negx};
-                precise = true;
-            } else {
-                sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L);
-                defer = sizeof(R) == 4 && (sw.mna <= P.near_band || f.mode == S_CROSS);
-            }
+        if (cached) {
+            // another region containing the point keeps the signed minimum negative
+            if (f.negx && sw.mn >= (R)0) sw.mn = (R)-1;
+        } else {
             f.cache = kNearestCache && !ADJ && P.cache_ok && f.mode != S_CROSS;
             f.nk = sw.k;
             f.negx = sw.negx;
@@ -1429,11 +1438,14 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
             if (i < total) {
                 const int s = s_list[i];
                 int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-                for (int r = 0; r < reps; ++r) {
+                for (int r = 0;; ++r) {
                     transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
                         P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc,
                         VAR ? vbase + (size_t)s * kVarSlotBytes : nullptr);
                     if (act == A_DONE) break;
+                    // a run of FP64 near-surface steps may continue in this pass
+                    const bool chain = kPreciseChain > 0 && act == A_PRECISE && f.near && r < kPreciseChain;
+                    if (r + 1 >= reps && !chain) break;
                 }
                 store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
             }
