@@ -20,7 +20,7 @@ module smcrt_c
     implicit none
     private :: c_strlen
 
-    integer(c_int32_t), parameter :: SMCRT_ABI_VERSION_EXPECTED = 3
+    integer(c_int32_t), parameter :: SMCRT_ABI_VERSION_EXPECTED = 4
 
     ! smcrt_status
     integer(c_int32_t), parameter :: SMCRT_OK = 0, SMCRT_ERR_ARG = 1, SMCRT_ERR_SCENE = 2, SMCRT_ERR_CUDA = 3, &
@@ -106,7 +106,7 @@ module smcrt_c
     type, bind(C) :: smcrt_tuning
         integer(c_int32_t) :: tally_copies, shared_bins
         real(c_double)     :: packets_per_s
-        integer(c_int32_t) :: trials, reserved
+        integer(c_int32_t) :: trials, block_size, slots_per_thread, ctas_per_sm
     end type smcrt_tuning
 
     type, bind(C) :: smcrt_region_optics

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define SMCRT_ABI_VERSION 3
+#define SMCRT_ABI_VERSION 4
 
 /* ---- status codes -------------------------------------------------------- */
 enum smcrt_status {
@@ -304,7 +304,9 @@ typedef struct smcrt_tuning {
     int32_t shared_bins;   /* 1: detector bins counted in shared memory */
     double packets_per_s;  /* measured rate of the chosen configuration */
     int32_t trials;        /* trial runs made */
-    int32_t reserved;
+    int32_t block_size;    /* threads per CTA of the transport kernel (fixed at build time) */
+    int32_t slots_per_thread; /* packet slots per thread (2 in FP32, 1 in FP64 transport) */
+    int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent grid */
 } smcrt_tuning;
 int32_t smcrt_autotune(smcrt_ctx* ctx, int64_t trial_packets, uint64_t seed, smcrt_tuning* result);
 

@@ -8,7 +8,7 @@ import ctypes as C
 
 import numpy as np
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 # status
 OK, ERR_ARG, ERR_SCENE, ERR_CUDA, ERR_DEVICE, ERR_TIMEOUT, ERR_NO_DEVICE = range(7)
@@ -132,7 +132,8 @@ class RegionOptics(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("tally_copies", C.c_int32), ("shared_bins", C.c_int32), ("packets_per_s", C.c_double),
-                ("trials", C.c_int32), ("reserved", C.c_int32)]
+                ("trials", C.c_int32), ("block_size", C.c_int32), ("slots_per_thread", C.c_int32),
+                ("ctas_per_sm", C.c_int32)]
 
 
 # Exported symbols of include/smcrt.h with their argtypes/restype.

@@ -852,7 +852,10 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
         result->shared_bins = best_sb;
         result->packets_per_s = best;
         result->trials = trials;
-        result->reserved = 0;
+        result->block_size = c->block;
+        result->slots_per_thread =
+            c->precision == SMCRT_FP64 ? SlotCount<double>::per_thread : SlotCount<float>::per_thread;
+        result->ctas_per_sm = c->grid_blocks / std::max(1, c->nsm);
     }
     return SMCRT_OK;
 }

@@ -150,7 +150,8 @@ class Transport:
         t = abi.Tuning()
         check(lib().smcrt_autotune(self._ctx, int(trial_packets), int(seed), C.byref(t)))
         return {"tally_copies": t.tally_copies, "shared_bins": bool(t.shared_bins),
-                "packets_per_s": t.packets_per_s, "trials": t.trials}
+                "packets_per_s": t.packets_per_s, "trials": t.trials, "block_size": t.block_size,
+                "slots_per_thread": t.slots_per_thread, "ctas_per_sm": t.ctas_per_sm}
 
     def run_device(self, first: int, count: int, seed: int, jmean_dev: int, bins_dev: int | None,
                    stats: bool = False) -> dict | None:

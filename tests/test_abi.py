@@ -69,7 +69,8 @@ STRUCTS = {
                                 "variance_overflows", "reserved2"]),
     "smcrt_packet_state": (abi.PacketState, ["pos", "dir", "weight", "layer", "nscatt", "ndraws", "flags"]),
     "smcrt_region_optics": (abi.RegionOptics, ["mus", "mua", "hgg", "n"]),
-    "smcrt_tuning": (abi.Tuning, ["tally_copies", "shared_bins", "packets_per_s", "trials"]),
+    "smcrt_tuning": (abi.Tuning, ["tally_copies", "shared_bins", "packets_per_s", "trials", "block_size",
+                                  "slots_per_thread", "ctas_per_sm"]),
 }
 
 

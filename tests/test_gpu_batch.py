@@ -87,6 +87,7 @@ def test_autotune_keeps_results(cfg):
         t = tr.autotune(trial_packets=50000)
         after = tr.run(20000, 4)
     assert t["tally_copies"] in (1, 2, 4, 8) and t["packets_per_s"] > 0 and t["trials"] >= 2
+    assert t["block_size"] == 640 and t["slots_per_thread"] == 1 and t["ctas_per_sm"] >= 1
     assert before.stats["voxel_segments"] == after.stats["voxel_segments"]
     assert np.array_equal(before.bins, after.bins)
     np.testing.assert_allclose(after.jmean, before.jmean, rtol=1e-9, atol=1e-12 * before.jmean.max())
