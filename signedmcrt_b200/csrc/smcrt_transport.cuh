@@ -281,12 +281,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define SMCRT_NEAREST_CACHE 1
 #endif
 constexpr bool kNearestCache = SMCRT_NEAREST_CACHE != 0;
-// FP32 transport: extra passes a packet may take within one round while it is on a
-// run of FP64 near-surface steps (0: none; each step waits for the next round)
-#ifndef SMCRT_PRECISE_CHAIN
-#define SMCRT_PRECISE_CHAIN 0
-#endif
-constexpr int kPreciseChain = SMCRT_PRECISE_CHAIN;
 
 // Per-lane actions of the flattened transport loop.
 // A_PRECISE (FP32 transport): a sweep within the FP64 band of a surface, or resolving a
@@ -1244,6 +1238,8 @@ __device__ __forceinline__ int load_slot(const Slots<R, ADJ>& sl, int s, const P
         f.x.oldpos.z = get_r<double>(sl.u, 4, s);
         f.x.which = (int)sl.u[6][s];
         f.x.nl = (int)sl.u[7][s];
+    } else if (act == A_SWEEP || act == A_PRECISE) {
+        f.dsdf = get_r<R>(sl.u, 4 * W, s);
     }
     return act;
 }
@@ -1296,6 +1292,8 @@ __device__ __forceinline__ void store_slot(Slots<R, ADJ>& sl, int s, int act, co
         put_r<double>(sl.u, 4, s, f.x.oldpos.z);
         sl.u[6][s] = (uint32_t)f.x.which;
         sl.u[7][s] = (uint32_t)f.x.nl;
+    } else if (act == A_SWEEP || act == A_PRECISE) {
+        put_r<R>(sl.u, 4 * W, s, f.dsdf);  // the last step's length (the cache's bound)
     }
 }
 
@@ -1438,14 +1436,11 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
             if (i < total) {
                 const int s = s_list[i];
                 int act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-                for (int r = 0;; ++r) {
+                for (int r = 0; r < reps; ++r) {
                     transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
                         P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc,
                         VAR ? vbase + (size_t)s * kVarSlotBytes : nullptr);
                     if (act == A_DONE) break;
-                    // a run of FP64 near-surface steps may continue in this pass
-                    const bool chain = kPreciseChain > 0 && act == A_PRECISE && f.near && r < kPreciseChain;
-                    if (r + 1 >= reps && !chain) break;
                 }
                 store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
             }
