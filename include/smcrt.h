@@ -208,8 +208,13 @@ typedef struct smcrt_options {
                               history-based second moment of jmean; see
                               smcrt_run_moments).  Needs a scene in the parameter
                               block; allocates a voxel-score table per packet slot
-                              (4 KiB each, ~0.8 GB for FP32 on 148 SMs) */
-    int32_t reserved[6];   /* zero */
+                              (40 KiB each, ~7.8 GB for FP32 on 148 SMs) */
+    int32_t nearest_cache; /* SDF sweeps of tracing steps skip the regions a per-packet
+                              nearest-region bound rules out (results unchanged):
+                              0 = library choice (scenes of 9 or more regions whose
+                              regions are exact distances under rigid transforms),
+                              1 = on where the scene allows it, 2 = off */
+    int32_t reserved[5];   /* zero */
 } smcrt_options;
 
 /* Event counters of one run (definitions identical in the CPU oracle). */
@@ -307,6 +312,8 @@ typedef struct smcrt_tuning {
     int32_t block_size;    /* threads per CTA of the transport kernel (fixed at build time) */
     int32_t slots_per_thread; /* packet slots per thread (2 in FP32, 1 in FP64 transport) */
     int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent grid */
+    int32_t nearest_cache; /* 1: sweeps skip regions the nearest-region cache rules out */
+    int32_t reserved;
 } smcrt_tuning;
 int32_t smcrt_autotune(smcrt_ctx* ctx, int64_t trial_packets, uint64_t seed, smcrt_tuning* result);
 

@@ -209,6 +209,9 @@ double near_band(double eps, const smcrt_grid& g) {
     return std::fmax(2.0 * eps, 16.0 * ulp);
 }
 
+// Scenes with at least this many regions use the nearest-region cache by default.
+constexpr int kCacheMinRegions = 9;
+
 // The per-flight sphere-trace step count shares its slot word with the
 // nearest-region cache: 21 bits.
 constexpr int kMaxTraceSteps = (1 << 21) - 1;
@@ -280,6 +283,7 @@ struct smcrt_ctx {
     unsigned char* d_vartab = nullptr;        // voxel-score table of every packet slot
     size_t vartab_bytes = 0;
     bool vartab_clean = false;                // every table seen empty after the last moments run
+    bool cache_allowed = false;               // every region 1-Lipschitz: the nearest-region cache may run
     double* d_jmean2 = nullptr;               // second moment of smcrt_run_moments
 };
 
@@ -353,7 +357,12 @@ void fill_params(Params<R>* P, const smcrt_scene* scene, const smcrt_grid* grid,
     const int prec = (sizeof(R) == 4) ? SMCRT_FP32 : SMCRT_FP64;
     P->eps = (R)((o && o->eps > 0) ? o->eps : default_eps(prec, *grid));
     P->near_band = (R)near_band((double)P->eps, *grid);
-    P->cache_ok = cache_policy(scene, grid, (int)sizeof(R), &P->cache_margin) ? 1 : 0;
+    // the nearest-region cache pays where a sweep has many regions to skip (on
+    // small scenes the lanes of a warp rarely all skip the same region, and the
+    // bookkeeping costs more than it saves); smcrt_autotune times both
+    const bool allowed = cache_policy(scene, grid, (int)sizeof(R), &P->cache_margin);
+    const int want = o ? o->nearest_cache : 0;
+    P->cache_ok = allowed && (want == 1 || (want == 0 && scene->nregions >= kCacheMinRegions)) ? 1 : 0;
     P->normal_h = (o && o->normal_h > 0) ? o->normal_h : 1e-6;
     P->instance = o ? o->instance : 0u;
     P->tcopies = 1;
@@ -610,6 +619,8 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
         return fail(SMCRT_ERR_ARG, "detectors: 0.." + std::to_string(kMaxDetectors) + " supported");
     if (opts && (opts->scene_memory < 0 || opts->scene_memory > 1))
         return fail(SMCRT_ERR_ARG, "options: scene_memory must be 0 or 1");
+    if (opts && (opts->nearest_cache < 0 || opts->nearest_cache > 2))
+        return fail(SMCRT_ERR_ARG, "options: nearest_cache must be 0, 1 or 2");
     const bool big = scene->nregions > kMaxRegions || scene->nprims > kMaxPrims || (opts && opts->scene_memory == 1);
     const int prec = opts ? opts->precision : SMCRT_FP32;
     const int kern = opts ? opts->kernel : SMCRT_KERNEL_PATHLENGTH;
@@ -639,6 +650,10 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
     c->timeout_ms = (opts && opts->timeout_ms > 0) ? opts->timeout_ms : 600000;
     if (prec == SMCRT_FP64) c->pd = make_params<double>(scene, grid, source, dtab, ndet, opts);
     else c->pf = make_params<float>(scene, grid, source, dtab, ndet, opts);
+    {
+        double margin;
+        c->cache_allowed = cache_policy(scene, grid, prec == SMCRT_FP64 ? 8 : 4, &margin);
+    }
 
     auto bail = [&](int code) {
         smcrt_destroy(c);
@@ -816,14 +831,22 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
     }
     std::vector<int> sbins = {1};
     if (c->nbins > 0 && c->nbins <= kMaxSharedBins) sbins.push_back(0);
+    std::vector<int> caches = {0};
+    if (c->cache_allowed) caches.push_back(1);
     const int keep_tc = c->tcopies;
     const bool keep_sb = c->shared_bins_on;
+    auto set_cache = [&](int on) {
+        if (c->pf) c->pf->cache_ok = on;
+        if (c->pd) c->pd->cache_ok = on;
+    };
     double best = -1.0;
-    int best_tc = keep_tc, best_sb = keep_sb, trials = 0;
+    int best_tc = keep_tc, best_sb = keep_sb, best_cache = c->pf ? c->pf->cache_ok : c->pd->cache_ok, trials = 0;
     for (int tc : copies)
-        for (int sb : sbins) {
+        for (int sb : sbins)
+          for (int ca : caches) {
             c->tcopies = tc;
             c->shared_bins_on = sb != 0;
+            set_cache(ca);
             double best_here = 0.0;
             for (int rep = 0; rep < 2; ++rep) {  // best of two: the first may pay cold caches
                 CK(cudaMemsetAsync(c->d_jmean, 0, sizeof(double) * c->ncell, c->stream));
@@ -843,10 +866,12 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
                 best = best_here;
                 best_tc = tc;
                 best_sb = sb;
+                best_cache = ca;
             }
         }
     c->tcopies = best_tc;
     c->shared_bins_on = best_sb != 0;
+    set_cache(best_cache);
     if (result) {
         result->tally_copies = best_tc;
         result->shared_bins = best_sb;
@@ -856,6 +881,7 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
         result->slots_per_thread =
             c->precision == SMCRT_FP64 ? SlotCount<double>::per_thread : SlotCount<float>::per_thread;
         result->ctas_per_sm = c->grid_blocks / std::max(1, c->nsm);
+        result->nearest_cache = best_cache;
     }
     return SMCRT_OK;
 }

@@ -361,7 +361,12 @@ __device__ __forceinline__ SweepOut<T> sweep_regions(const S& sc, V3<T> p, int L
     T inner = (T)INFINITY;
     int nneg = 0;
     bool kneg = false;
-    for (int i = 0; i < sc.nregions; ++i) {
+    // the warp's range of regions: all of them when a lane sweeps in full, else
+    // from the lowest to the highest cached region of its lanes
+    const unsigned am = __activemask();
+    const int lo = __reduce_min_sync(am, (unsigned)(only >= 0 ? only : 0));
+    const int hi = __reduce_max_sync(am, (unsigned)(only >= 0 ? only : sc.nregions - 1));
+    for (int i = lo; i <= hi; ++i) {
         if (only >= 0 && i != only) continue;
         if constexpr (!std::is_same<S, SceneT<T>>::value) {
             const T br = sc.bound[4 * i + 3];

@@ -37,7 +37,8 @@ class Transport:
     def __init__(self, array, settings: Settings, *, kernel: str = "pathlength", precision: str = "fp32",
                  end_early: bool = False, stream: int | None = None, block_size: int = 0, blocks_per_sm: int = 0,
                  eps: float = 0.0, normal_h: float = 0.0, max_trace_steps: int = 0, timeout_ms: int = 0,
-                 instance: int = 0, tally_copies: int = 0, scene_memory: int = 0, variance: bool = False):
+                 instance: int = 0, tally_copies: int = 0, scene_memory: int = 0, variance: bool = False,
+                 nearest_cache: int = 0):
         self.settings = settings
         self.flat = array if isinstance(array, FlatScene) else FlatScene(array)
         self.grid = settings.grid_c()
@@ -57,6 +58,7 @@ class Transport:
         o.tally_copies = tally_copies  # 0: library choice; 1: a single fluence grid
         o.scene_memory = scene_memory  # 1: the scene from device memory even when it fits the parameter block
         o.variance = int(bool(variance))  # keep the per-voxel second moment (run_moments)
+        o.nearest_cache = nearest_cache  # 0: library choice; 1: on where allowed; 2: off
         # stream=None: a stream private to this context; an int: that cudaStream_t (0 = default)
         o.stream = stream if stream is not None else None
         o.private_stream = int(stream is None)
@@ -151,7 +153,8 @@ class Transport:
         check(lib().smcrt_autotune(self._ctx, int(trial_packets), int(seed), C.byref(t)))
         return {"tally_copies": t.tally_copies, "shared_bins": bool(t.shared_bins),
                 "packets_per_s": t.packets_per_s, "trials": t.trials, "block_size": t.block_size,
-                "slots_per_thread": t.slots_per_thread, "ctas_per_sm": t.ctas_per_sm}
+                "slots_per_thread": t.slots_per_thread, "ctas_per_sm": t.ctas_per_sm,
+                "nearest_cache": bool(t.nearest_cache)}
 
     def run_device(self, first: int, count: int, seed: int, jmean_dev: int, bins_dev: int | None,
                    stats: bool = False) -> dict | None:

@@ -61,3 +61,22 @@ def test_device_memory_scene_equals_parameter_block(gpu, cfg):
     assert not diff, diff
     fluence_agrees(rb.jmean, ra.jmean)
     assert np.array_equal(ra.bins, rb.bins)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("cfg,n", [("sphere_scene", 40), ("layered_vessels", 0), ("sphere_water", 0)])
+def test_nearest_region_cache_changes_nothing(gpu, cfg, n, precision):
+    """The nearest-region cache only skips regions that cannot be the nearest, and
+    the region it keeps is evaluated by the same code: runs with it on and off
+    follow identical histories -- identical event counters, the same fluence (up
+    to the order of the FP64 atomic adds) -- in FP64 and in FP32."""
+    st = P.sphere_scene_settings(num_spheres=n) if cfg == "sphere_scene" else P.benchmark_settings(cfg)
+    arr = P.setup_simulation(st)
+    out = []
+    for mode in (1, 2):
+        with gpu.Transport(arr, st, precision=precision, nearest_cache=mode) as tr:
+            out.append(tr.run(20000, 5))
+    on, off = out
+    for k in ("sdf_evals", "voxel_segments", "trace_steps", "scatters", "fresnel_events", "reflections"):
+        assert on.stats[k] == off.stats[k], (k, on.stats[k], off.stats[k])
+    np.testing.assert_allclose(on.jmean, off.jmean, rtol=1e-9, atol=1e-12 * off.jmean.max())
