@@ -70,6 +70,13 @@ struct Pk {
     bool tflag;
 };
 
+// Code on rare paths (emission, detector hits, the normal and region values of a
+// boundary event): inlined (default) or compiled as called functions, which keeps
+// the hot loop's code smaller at the cost of a call.
+#ifndef SMCRT_COLD
+#define SMCRT_COLD __forceinline__
+#endif
+
 template <class R>
 __device__ __forceinline__ V3<R> cv(V3<double> p) {
     return V3<R>{(R)p.x, (R)p.y, (R)p.z};
@@ -81,7 +88,7 @@ __device__ __forceinline__ V3<double> advance(V3<double> p, R d, V3<R> dir) {
 
 // Emitters, src/photon.f90
 template <class R, class Rng>
-__device__ __forceinline__ void emit(const Params<R>& P, Pk<R>& pk, Rng& rng) {
+__device__ SMCRT_COLD void emit(const Params<R>& P, Pk<R>& pk, Rng& rng) {
     const SourceT<R>& s = P.src;
     pk.tflag = false;
     pk.bounces = 0;
@@ -208,7 +215,7 @@ __device__ __forceinline__ long long detector_bin(const DetT& D, const double p[
 // Detector hits at packet death (kernelsMod.f90:302-306).  Each hit adds one
 // count; with privatized bins the count goes to the CTA's shared-memory copy.
 template <class R>
-__device__ __forceinline__ void record_detectors(const Params<R>& P, double* bins, unsigned* sbins, double px,
+__device__ SMCRT_COLD void record_detectors(const Params<R>& P, double* bins, unsigned* sbins, double px,
                                                  double py, double pz, double lx, double ly, double lz,
                                                  double weight, int layer1) {
     const double p[3] = {px, py, pz};
@@ -413,11 +420,11 @@ __device__ __forceinline__ SweepOut<T> sweep_regions(const S& sc, V3<T> p, int L
 // out-of-line function would receive the parameter block by reference and read
 // it through generic loads instead of the constant bank.
 template <class R, bool MODS, class S>
-__device__ __forceinline__ R eval_region_cold(const S& sc, int r, V3<R> p) {
+__device__ SMCRT_COLD R eval_region_cold(const S& sc, int r, V3<R> p) {
     return eval_region<R, MODS, S>(sc, r, p);
 }
 template <bool MODS, class S>
-__device__ __forceinline__ V3<double> calc_normal_cold(const S& sc, int r, V3<double> p, double h) {
+__device__ SMCRT_COLD V3<double> calc_normal_cold(const S& sc, int r, V3<double> p, double h) {
     return calc_normal<MODS, S>(sc, r, p, h);
 }
 
@@ -928,14 +935,24 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         const bool cached = kNearestCache && !ADJ && f.cache && f.mode == S_STEP &&
                             (double)(2 * f.dsdf) + P.cache_margin < (double)f.clear;
         const int only = cached ? f.nk : -1;
-        if (sizeof(R) == 4 && act == A_PRECISE) {
+        // FP64 at once: the FP64 group, or a tracing step right after an FP64 sweep
+        // that found the surface within half of near_band (f.near)
+        bool want64 = sizeof(R) == 4 && (act == A_PRECISE || (f.near && f.mode == S_STEP));
+        if (!want64) {
+            sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L, only);
+            defer = sizeof(R) == 4 && (sw.mna <= P.near_band || f.mode == S_CROSS);
+            // a lane on the cache has one region to evaluate in FP64: it does so
+            // now instead of waiting a round for the FP64 group (same values)
+            if (defer && cached) {
+                defer = false;
+                want64 = true;
+            }
+        }
+        if (want64) {
             const SweepOut<double> s64 = sweep_regions<double, MODS, S64>(sc64, pk.pos, L, only);
             sw = SweepOut<R>{(R)s64.mn, (R)s64.mna, (R)s64.d0, (R)s64.dsL, (R)s64.dsN, s64.nl, s64.lay,
                              (R)s64.m2, s64.k, s64.negx};
             precise = true;
-        } else {
-            sw = sweep_regions<R, MODS, S>(sc, cv<R>(pk.pos), L, only);
-            defer = sizeof(R) == 4 && (sw.mna <= P.near_band || f.mode == S_CROSS);
         }
         if (cached) {
             // another region containing the point keeps the signed minimum negative
@@ -1084,7 +1101,9 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
                 act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
             } else {
                 f.mode = S_STEP;
-                act = (sizeof(R) == 4 && f.near) ? A_PRECISE : A_SWEEP;
+                // near a surface the next sweep is FP64: in the FP64 group, or (a
+                // lane on the cache, one region) in its own next pass
+                act = (sizeof(R) == 4 && f.near && !f.cache) ? A_PRECISE : A_SWEEP;
             }
         }
     }
