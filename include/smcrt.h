@@ -211,9 +211,8 @@ typedef struct smcrt_options {
                               (40 KiB each, ~7.8 GB for FP32 on 148 SMs) */
     int32_t nearest_cache; /* SDF sweeps of tracing steps skip the regions a per-packet
                               nearest-region bound rules out (results unchanged):
-                              0 = library choice (scenes of 9 or more regions whose
-                              regions are exact distances under rigid transforms),
-                              1 = on where the scene allows it, 2 = off */
+                              0 or 1 = on where the scene allows it (every region an
+                              exact distance under a rigid transform), 2 = off */
     int32_t reserved[5];   /* zero */
 } smcrt_options;
 

@@ -209,9 +209,6 @@ double near_band(double eps, const smcrt_grid& g) {
     return std::fmax(2.0 * eps, 16.0 * ulp);
 }
 
-// Scenes with at least this many regions use the nearest-region cache by default.
-constexpr int kCacheMinRegions = 9;
-
 // The per-flight sphere-trace step count shares its slot word with the
 // nearest-region cache: 21 bits.
 constexpr int kMaxTraceSteps = (1 << 21) - 1;
@@ -357,12 +354,11 @@ void fill_params(Params<R>* P, const smcrt_scene* scene, const smcrt_grid* grid,
     const int prec = (sizeof(R) == 4) ? SMCRT_FP32 : SMCRT_FP64;
     P->eps = (R)((o && o->eps > 0) ? o->eps : default_eps(prec, *grid));
     P->near_band = (R)near_band((double)P->eps, *grid);
-    // the nearest-region cache pays where a sweep has many regions to skip (on
-    // small scenes the lanes of a warp rarely all skip the same region, and the
-    // bookkeeping costs more than it saves); smcrt_autotune times both
+    // the nearest-region cache: on wherever every region is 1-Lipschitz, unless
+    // switched off (smcrt_autotune times both)
     const bool allowed = cache_policy(scene, grid, (int)sizeof(R), &P->cache_margin);
     const int want = o ? o->nearest_cache : 0;
-    P->cache_ok = allowed && (want == 1 || (want == 0 && scene->nregions >= kCacheMinRegions)) ? 1 : 0;
+    P->cache_ok = allowed && want != 2 ? 1 : 0;
     P->normal_h = (o && o->normal_h > 0) ? o->normal_h : 1e-6;
     P->instance = o ? o->instance : 0u;
     P->tcopies = 1;

@@ -70,13 +70,6 @@ struct Pk {
     bool tflag;
 };
 
-// Code on rare paths (emission, detector hits, the normal and region values of a
-// boundary event): inlined (default) or compiled as called functions, which keeps
-// the hot loop's code smaller at the cost of a call.
-#ifndef SMCRT_COLD
-#define SMCRT_COLD __forceinline__
-#endif
-
 template <class R>
 __device__ __forceinline__ V3<R> cv(V3<double> p) {
     return V3<R>{(R)p.x, (R)p.y, (R)p.z};
@@ -88,7 +81,7 @@ __device__ __forceinline__ V3<double> advance(V3<double> p, R d, V3<R> dir) {
 
 // Emitters, src/photon.f90
 template <class R, class Rng>
-__device__ SMCRT_COLD void emit(const Params<R>& P, Pk<R>& pk, Rng& rng) {
+__device__ __forceinline__ void emit(const Params<R>& P, Pk<R>& pk, Rng& rng) {
     const SourceT<R>& s = P.src;
     pk.tflag = false;
     pk.bounces = 0;
@@ -215,7 +208,7 @@ __device__ __forceinline__ long long detector_bin(const DetT& D, const double p[
 // Detector hits at packet death (kernelsMod.f90:302-306).  Each hit adds one
 // count; with privatized bins the count goes to the CTA's shared-memory copy.
 template <class R>
-__device__ SMCRT_COLD void record_detectors(const Params<R>& P, double* bins, unsigned* sbins, double px,
+__device__ __forceinline__ void record_detectors(const Params<R>& P, double* bins, unsigned* sbins, double px,
                                                  double py, double pz, double lx, double ly, double lz,
                                                  double weight, int layer1) {
     const double p[3] = {px, py, pz};
@@ -288,6 +281,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define SMCRT_NEAREST_CACHE 1
 #endif
 constexpr bool kNearestCache = SMCRT_NEAREST_CACHE != 0;
+// ... also for the sweep at a flight's start (after a scatter)
+#ifndef SMCRT_CACHE_TOP
+#define SMCRT_CACHE_TOP 1
+#endif
+constexpr bool kCacheTop = SMCRT_CACHE_TOP != 0;
 
 // Per-lane actions of the flattened transport loop.
 // A_PRECISE (FP32 transport): a sweep within the FP64 band of a surface, or resolving a
@@ -315,6 +313,7 @@ struct Flight {
     bool cache, negx;
     int nk;
     float clear;
+    float dkup;  // an upper bound on region k's |d| at the current position
     // FP32 transport: the last sweep was taken in FP64 and found the surface
     // within half of near_band, so the next step's sweep is within near_band too
     // (a move of min|d| changes every |d| by at most that) and goes straight to FP64
@@ -333,6 +332,13 @@ struct Flight {
         } x;
     };
 };
+
+// A move of f.dsdf: off the clearance, onto the bound on |d_k|.
+template <class R>
+__device__ __forceinline__ void cache_move(Flight<R>& f) {
+    f.clear = __fsub_rd(f.clear, float_ru(f.dsdf));
+    f.dkup = __fadd_ru(f.dkup, float_ru(f.dsdf));
+}
 
 // All regions at one point (the sweep of tauint2, inttau2.f90:51-55,86-96,104-108):
 // signed minimum, minimum |d|, region 0's value, region L's value, the first
@@ -420,11 +426,11 @@ __device__ __forceinline__ SweepOut<T> sweep_regions(const S& sc, V3<T> p, int L
 // out-of-line function would receive the parameter block by reference and read
 // it through generic loads instead of the constant bank.
 template <class R, bool MODS, class S>
-__device__ SMCRT_COLD R eval_region_cold(const S& sc, int r, V3<R> p) {
+__device__ __forceinline__ R eval_region_cold(const S& sc, int r, V3<R> p) {
     return eval_region<R, MODS, S>(sc, r, p);
 }
 template <bool MODS, class S>
-__device__ SMCRT_COLD V3<double> calc_normal_cold(const S& sc, int r, V3<double> p, double h) {
+__device__ __forceinline__ V3<double> calc_normal_cold(const S& sc, int r, V3<double> p, double h) {
     return calc_normal<MODS, S>(sc, r, p, h);
 }
 
@@ -708,7 +714,7 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
     if (a < 0) {
         if (ADJ) adj_track(P, pk, acc, (float)f.dsdf, 0.0f);  // a step outside the grid
         pk.pos = advance(pk.pos, f.dsdf, pk.dir);
-        f.clear = __fsub_rd(f.clear, float_ru(f.dsdf));
+        cache_move(f);
         if (f.last) return end_flight(P, pk);
         f.mode = S_STEP;
         return A_SWEEP;
@@ -929,11 +935,10 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
         const int L = pk.layer;
         SweepOut<R> sw{};
         bool precise = false, defer = false;
-        // the cache holds for a tracing step when |d_k| + margin stays below the
-        // clearance: |d_k| was the step length f.dsdf before the move, so it is
-        // at most 2 f.dsdf now (the move is already off the clearance)
-        const bool cached = kNearestCache && !ADJ && f.cache && f.mode == S_STEP &&
-                            (double)(2 * f.dsdf) + P.cache_margin < (double)f.clear;
+        // the cache holds for a tracing step or a flight start when the bound on
+        // |d_k| plus the margin stays below the clearance
+        const bool cached = kNearestCache && !ADJ && f.cache && (f.mode == S_STEP || (kCacheTop && f.mode == S_TOP)) &&
+                            (double)f.dkup + P.cache_margin < (double)f.clear;
         const int only = cached ? f.nk : -1;
         // FP64 at once: the FP64 group, or a tracing step right after an FP64 sweep
         // that found the surface within half of near_band (f.near)
@@ -963,6 +968,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
             f.negx = sw.negx;
             f.clear = float_rd(sw.m2);
         }
+        f.dkup = float_ru(sw.mna);  // |d_k| here: the minimum found
         if (defer) {
             f.near = false;
             act = A_PRECISE;
@@ -1096,7 +1102,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
         if (walk_segment<R, BATCH, ADJ, VAR>(P, pk, f, c, acc, vt)) {
             pk.pos = advance(pk.pos, f.dsdf, pk.dir);
-            f.clear = __fsub_rd(f.clear, float_ru(f.dsdf));
+            cache_move(f);
             if (f.last) {
                 act = end_flight(P, pk);  // taurun >= tau ends the flight (:100)
             } else {
@@ -1163,7 +1169,8 @@ struct Slots {
     // trace steps | nearest region << 21 | negx << 29 | cache valid << 30 | near << 31
     uint32_t steps[kSlots];
     int nscatt[kSlots];
-    float clr[ADJ ? 1 : kSlots];  // nearest-region cache clearance (not in adjoint launches)
+    // nearest-region cache: clearance and the bound on |d_k| (not in adjoint launches)
+    float clr[ADJ ? 1 : kSlots], dku[ADJ ? 1 : kSlots];
     uint32_t bl[kSlots];  // bounces (<= 1001) | rng.left << 11 | batch instance << 14
     // Philox block counter (replay builds: the injected uniforms consumed); the
     // draw count of a Philox stream is 4 words a block less the words left
@@ -1216,6 +1223,7 @@ __device__ __forceinline__ int load_slot(const Slots<R, ADJ>& sl, int s, const P
     f.cache = !ADJ && ((sw >> 30) & 1u);
     f.near = (sw >> 31) & 1u;
     f.clear = ADJ ? 0.0f : sl.clr[ADJ ? 0 : s];
+    f.dkup = ADJ ? 0.0f : sl.dku[ADJ ? 0 : s];
     pk.nscatt = sl.nscatt[s];
     const uint32_t bl = sl.bl[s];
     pk.bounces = (int)(bl & 0x7FFu);
@@ -1262,8 +1270,6 @@ __device__ __forceinline__ int load_slot(const Slots<R, ADJ>& sl, int s, const P
         f.x.oldpos.z = get_r<double>(sl.u, 4, s);
         f.x.which = (int)sl.u[6][s];
         f.x.nl = (int)sl.u[7][s];
-    } else if (act == A_SWEEP || act == A_PRECISE) {
-        f.dsdf = get_r<R>(sl.u, 4 * W, s);
     }
     return act;
 }
@@ -1286,7 +1292,10 @@ __device__ __forceinline__ void store_slot(Slots<R, ADJ>& sl, int s, int act, co
     sl.taurun[s] = f.taurun;
     sl.steps[s] = (uint32_t)f.steps | ((uint32_t)f.nk << 21) | ((uint32_t)f.negx << 29) |
                   ((uint32_t)(!ADJ && f.cache) << 30) | ((uint32_t)f.near << 31);
-    if (!ADJ) sl.clr[ADJ ? 0 : s] = f.clear;
+    if (!ADJ) {
+        sl.clr[ADJ ? 0 : s] = f.clear;
+        sl.dku[ADJ ? 0 : s] = f.dkup;
+    }
     sl.nscatt[s] = pk.nscatt;
     sl.bl[s] = (uint32_t)pk.bounces | ((uint32_t)rng.left << 11) | ((uint32_t)(BATCH ? pk.inst : 0) << 14);
     sl.p0[s] = rng.p0;
@@ -1316,8 +1325,6 @@ __device__ __forceinline__ void store_slot(Slots<R, ADJ>& sl, int s, int act, co
         put_r<double>(sl.u, 4, s, f.x.oldpos.z);
         sl.u[6][s] = (uint32_t)f.x.which;
         sl.u[7][s] = (uint32_t)f.x.nl;
-    } else if (act == A_SWEEP || act == A_PRECISE) {
-        put_r<R>(sl.u, 4 * W, s, f.dsdf);  // the last step's length (the cache's bound)
     }
 }
 
