@@ -499,6 +499,8 @@ def main() -> None:
     ap.add_argument("--eps", type=float, default=0.0, help="surface epsilon (default: the library's, 1e-8)")
     ap.add_argument("--nearest-cache", type=int, default=0, choices=(0, 1, 2),
                     help="nearest-region sweep cache: 0 library choice, 1 on, 2 off")
+    ap.add_argument("--shared-fluence", type=int, default=0, choices=(0, 1, 2),
+                    help="shared-memory beam sub-box of the fluence (FP32 pencil beams): 0 library choice, 1 on, 2 off")
     ap.add_argument("--num-spheres", type=int, default=40,
                     help="sphere_scene: spheres of the reference's res/sphere.toml scene (regions = this + 1)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample length")
@@ -561,7 +563,7 @@ def main() -> None:
     stream = torch.cuda.Stream(dev)  # every timed launch goes to this stream
     torch.cuda.set_stream(stream)
     tr = T.Transport(flat, st, precision=args.precision, stream=stream.cuda_stream, timeout_ms=600000,
-                     eps=args.eps, nearest_cache=args.nearest_cache)
+                     eps=args.eps, nearest_cache=args.nearest_cache, shared_fluence=args.shared_fluence)
     jm = torch.zeros(tr.ncell, dtype=torch.float64, device=dev)
     bins = torch.zeros(max(tr.nbins, 1), dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
@@ -617,7 +619,7 @@ def main() -> None:
         jh = torch.empty(tr.ncell, dtype=torch.float64, pin_memory=True).numpy()
         bh = torch.empty(max(tr.nbins, 1), dtype=torch.float64, pin_memory=True).numpy()
         tr_host = T.Transport(flat, st, precision=args.precision, timeout_ms=600000, eps=args.eps,
-                              nearest_cache=args.nearest_cache)
+                              nearest_cache=args.nearest_cache, shared_fluence=args.shared_fluence)
         tr_host.run(min(per_gpu, 100000), 1, jmean_out=jh, bins_out=bh[:tr_host.nbins] if tr_host.nbins else None)
         if world > 1:
             dist.barrier()

@@ -86,7 +86,7 @@ module smcrt_c
         integer(c_int32_t) :: instance, timeout_ms
         type(c_ptr)        :: stream
         integer(c_int32_t) :: private_stream, tally_copies, scene_memory, variance, nearest_cache
-        integer(c_int32_t) :: reserved(5)
+        integer(c_int32_t) :: shared_fluence, reserved(4)
     end type smcrt_options
 
     type, bind(C) :: smcrt_stats
@@ -106,7 +106,7 @@ module smcrt_c
     type, bind(C) :: smcrt_tuning
         integer(c_int32_t) :: tally_copies, shared_bins
         real(c_double)     :: packets_per_s
-        integer(c_int32_t) :: trials, block_size, slots_per_thread, ctas_per_sm, nearest_cache, reserved
+        integer(c_int32_t) :: trials, block_size, slots_per_thread, ctas_per_sm, nearest_cache, shared_fluence
     end type smcrt_tuning
 
     type, bind(C) :: smcrt_region_optics

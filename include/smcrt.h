@@ -213,7 +213,13 @@ typedef struct smcrt_options {
                               nearest-region bound rules out (results unchanged):
                               0 or 1 = on where the scene allows it (every region an
                               exact distance under a rigid transform), 2 = off */
-    int32_t reserved[5];   /* zero */
+    int32_t shared_fluence; /* FP32 transport with a pencil source: each CTA sums the
+                              fluence of a sub-box along the beam (8 x 8 cells across it,
+                              as far along it as shared memory allows) in shared memory
+                              as 64-bit fixed point (2^-32 cm) and adds it to the FP64
+                              grid once; 0 = library choice (off unless smcrt_autotune
+                              picks it), 1 = on, 2 = off */
+    int32_t reserved[4];   /* zero */
 } smcrt_options;
 
 /* Event counters of one run (definitions identical in the CPU oracle). */
@@ -312,7 +318,7 @@ typedef struct smcrt_tuning {
     int32_t slots_per_thread; /* packet slots per thread (2 in FP32, 1 in FP64 transport) */
     int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent grid */
     int32_t nearest_cache; /* 1: sweeps skip regions the nearest-region cache rules out */
-    int32_t reserved;
+    int32_t shared_fluence; /* 1: each CTA sums a beam-axis sub-box of the fluence in shared memory */
 } smcrt_tuning;
 int32_t smcrt_autotune(smcrt_ctx* ctx, int64_t trial_packets, uint64_t seed, smcrt_tuning* result);
 

@@ -69,7 +69,7 @@ class Options(C.Structure):
                 ("eps", C.c_double), ("normal_h", C.c_double), ("instance", C.c_uint32),
                 ("timeout_ms", C.c_int32), ("stream", C.c_void_p), ("private_stream", C.c_int32),
                 ("tally_copies", C.c_int32), ("scene_memory", C.c_int32), ("variance", C.c_int32),
-                ("nearest_cache", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("nearest_cache", C.c_int32), ("shared_fluence", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class Stats(C.Structure):
@@ -133,7 +133,7 @@ class RegionOptics(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("tally_copies", C.c_int32), ("shared_bins", C.c_int32), ("packets_per_s", C.c_double),
                 ("trials", C.c_int32), ("block_size", C.c_int32), ("slots_per_thread", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("nearest_cache", C.c_int32), ("reserved", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("nearest_cache", C.c_int32), ("shared_fluence", C.c_int32)]
 
 
 # Exported symbols of include/smcrt.h with their argtypes/restype.

@@ -281,6 +281,10 @@ struct smcrt_ctx {
     size_t vartab_bytes = 0;
     bool vartab_clean = false;                // every table seen empty after the last moments run
     bool cache_allowed = false;               // every region 1-Lipschitz: the nearest-region cache may run
+    // shared-memory fluence privatisation (FP32, sources with a start point): the
+    // sub-box around the source's cell, its extent along the beam fitted per launch
+    bool priv_allowed = false, priv_on = false;
+    int priv_o[3] = {0, 0, 0}, priv_d[3] = {0, 0, 0}, priv_axis = 2, priv_sign = -1;
     double* d_jmean2 = nullptr;               // second moment of smcrt_run_moments
 };
 
@@ -412,6 +416,31 @@ void set_tally_table(Params<R>* P, double* jm, double* copies, int tc, long long
         P->jtab[k] = (k == 0) ? jm : (k < tc ? copies + (long long)(k - 1) * ncell : nullptr);
 }
 
+// The privatised sub-box of a launch with `sb` shared detector bins: the context's
+// box, its extent along the beam cut to the shared memory left beside the slots
+// and the bins (no box when fewer than 64 cells fit).
+int set_priv(smcrt_ctx* c, Params<float>& P, int sb) {
+    P.priv_n = 0;
+    if (!c->priv_on) return SMCRT_OK;
+    int cells = 0;
+    cudaError_t e = c->kernel == SMCRT_KERNEL_WEIGHT ? priv_cells_f32_1(sb, &cells)
+                  : c->kernel == SMCRT_KERNEL_TEST ? priv_cells_f32_2(sb, &cells)
+                                                   : priv_cells_f32_0(sb, &cells);
+    if (e != cudaSuccess) return fail(SMCRT_ERR_CUDA, std::string("shared fluence: ") + cudaGetErrorString(e));
+    int d[3] = {c->priv_d[0], c->priv_d[1], c->priv_d[2]};
+    const int a = c->priv_axis, across = d[(a + 1) % 3] * d[(a + 2) % 3];
+    d[a] = std::min(d[a], cells / std::max(1, across));
+    if (d[a] < 1 || d[0] * d[1] * d[2] < 64) return SMCRT_OK;
+    int o[3] = {c->priv_o[0], c->priv_o[1], c->priv_o[2]};
+    if (c->priv_sign < 0) o[a] = c->priv_o[a] + c->priv_d[a] - d[a];  // keep the cells next to the source
+    for (int k = 0; k < 3; ++k) {
+        P.priv_o[k] = o[k];
+        P.priv_d[k] = d[k];
+    }
+    P.priv_n = d[0] * d[1] * d[2];
+    return SMCRT_OK;
+}
+
 // Enqueues: reset work/counters/status, then the kernel for [first, first+count).
 // jm2: the second-moment grid of a moments run (nullptr otherwise).  Retiring
 // packets empty their voxel-score tables, so the tables are filled with the empty
@@ -450,6 +479,8 @@ int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, doubl
         c->pf->sbins = sb;
         c->pf->var_tab = jm2 ? c->d_vartab : nullptr;
         c->pf->jmean2 = jm2;
+        rc = set_priv(c, *c->pf, sb);
+        if (rc) return rc;
         set_tally_table(c->pf, jm, c->d_copies, tc, c->ncell);
         rc = launch_f32(c, *c->pf, B, replay, blocks);
     }
@@ -617,6 +648,8 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
         return fail(SMCRT_ERR_ARG, "options: scene_memory must be 0 or 1");
     if (opts && (opts->nearest_cache < 0 || opts->nearest_cache > 2))
         return fail(SMCRT_ERR_ARG, "options: nearest_cache must be 0, 1 or 2");
+    if (opts && (opts->shared_fluence < 0 || opts->shared_fluence > 2))
+        return fail(SMCRT_ERR_ARG, "options: shared_fluence must be 0, 1 or 2");
     const bool big = scene->nregions > kMaxRegions || scene->nprims > kMaxPrims || (opts && opts->scene_memory == 1);
     const int prec = opts ? opts->precision : SMCRT_FP32;
     const int kern = opts ? opts->kernel : SMCRT_KERNEL_PATHLENGTH;
@@ -649,6 +682,31 @@ int32_t smcrt_create(const smcrt_scene* scene, const smcrt_grid* grid, const smc
     {
         double margin;
         c->cache_allowed = cache_policy(scene, grid, prec == SMCRT_FP64 ? 8 : 4, &margin);
+    }
+    // the privatised fluence sub-box of a pencil beam: 8 x 8 cells around the
+    // entry cell across the beam, along it from the entry through the grid
+    if (prec == SMCRT_FP32 && source->kind == SMCRT_SRC_PENCIL) {
+        const double mx[3] = {grid->xmax, grid->ymax, grid->zmax};
+        const int n[3] = {grid->nxg, grid->nyg, grid->nzg};
+        int cell[3], axis = 0;
+        for (int a = 0; a < 3; ++a) {
+            const int ca = (int)std::floor((source->pos[a] + mx[a]) * n[a] / (2.0 * mx[a]));
+            cell[a] = std::min(std::max(ca, 0), n[a] - 1);
+            if (std::fabs(source->dir[a]) > std::fabs(source->dir[axis])) axis = a;
+        }
+        c->priv_axis = axis;
+        c->priv_sign = source->dir[axis] > 0 ? 1 : -1;
+        for (int a = 0; a < 3; ++a) {
+            if (a == axis) {
+                c->priv_o[a] = c->priv_sign > 0 ? cell[a] : 0;
+                c->priv_d[a] = c->priv_sign > 0 ? n[a] - cell[a] : cell[a] + 1;
+            } else {
+                c->priv_d[a] = std::min(8, n[a]);
+                c->priv_o[a] = std::min(std::max(cell[a] - c->priv_d[a] / 2, 0), n[a] - c->priv_d[a]);
+            }
+        }
+        c->priv_allowed = true;
+        c->priv_on = opts && opts->shared_fluence == 1;
     }
 
     auto bail = [&](int code) {
@@ -787,6 +845,7 @@ int32_t smcrt_adjoint(smcrt_ctx* c, int64_t nphotons, uint64_t seed, const float
     P.count = nphotons;
     P.seed = seed;
     P.sbins = 0;
+    P.priv_n = 0;  // the adjoint keeps no fluence tally
     set_tally_table(&P, c->d_jmean, c->d_copies, 1, c->ncell);
     if (cudaMemsetAsync(c->d_work, 0, sizeof(unsigned long long) * (1 + C_NUM), c->stream) != cudaSuccess ||
         cudaMemsetAsync(c->d_mom, 0, sizeof(double) * 25, c->stream) != cudaSuccess ||
@@ -829,6 +888,8 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
     if (c->nbins > 0 && c->nbins <= kMaxSharedBins) sbins.push_back(0);
     std::vector<int> caches = {0};
     if (c->cache_allowed) caches.push_back(1);
+    std::vector<int> privs = {0};
+    if (c->priv_allowed) privs.push_back(1);
     const int keep_tc = c->tcopies;
     const bool keep_sb = c->shared_bins_on;
     auto set_cache = [&](int on) {
@@ -837,12 +898,15 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
     };
     double best = -1.0;
     int best_tc = keep_tc, best_sb = keep_sb, best_cache = c->pf ? c->pf->cache_ok : c->pd->cache_ok, trials = 0;
+    int best_priv = c->priv_on;
     for (int tc : copies)
         for (int sb : sbins)
-          for (int ca : caches) {
+          for (int ca : caches)
+            for (int pv : privs) {
             c->tcopies = tc;
             c->shared_bins_on = sb != 0;
             set_cache(ca);
+            c->priv_on = pv != 0;
             double best_here = 0.0;
             for (int rep = 0; rep < 2; ++rep) {  // best of two: the first may pay cold caches
                 CK(cudaMemsetAsync(c->d_jmean, 0, sizeof(double) * c->ncell, c->stream));
@@ -863,11 +927,13 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
                 best_tc = tc;
                 best_sb = sb;
                 best_cache = ca;
+                best_priv = pv;
             }
         }
     c->tcopies = best_tc;
     c->shared_bins_on = best_sb != 0;
     set_cache(best_cache);
+    c->priv_on = best_priv != 0;
     if (result) {
         result->tally_copies = best_tc;
         result->shared_bins = best_sb;
@@ -878,6 +944,7 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
             c->precision == SMCRT_FP64 ? SlotCount<double>::per_thread : SlotCount<float>::per_thread;
         result->ctas_per_sm = c->grid_blocks / std::max(1, c->nsm);
         result->nearest_cache = best_cache;
+        result->shared_fluence = best_priv;
     }
     return SMCRT_OK;
 }

@@ -540,6 +540,11 @@ struct Params {
     // margin of its test (FP32 transport: the FP32 sweeps' margin for both sweeps)
     int cache_ok;
     double cache_margin;
+    // shared-memory fluence privatisation (FP32 plain launches): a sub-box of
+    // voxels (0-based origin, extents; priv_n cells, 0 = off) whose segments each
+    // CTA sums in shared memory as 64-bit fixed point and adds to the grid once
+    int priv_n;
+    int priv_o[3], priv_d[3];
     double normal_h;
     unsigned long long seed;
     unsigned long long budget_ns;  // per-launch device time budget (0 = none)

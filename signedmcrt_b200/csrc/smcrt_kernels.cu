@@ -29,7 +29,7 @@ static cudaError_t allow_smem(K kernel, size_t bytes) {
 cudaError_t SMCRT_CAT(launch, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>& P, const Buffers& B, bool replay, int blocks,
                                                    int block, cudaStream_t s) {
     if (block != kBlock) return cudaErrorInvalidConfiguration;
-    const size_t smem = slots_bytes<SMCRT_R>() + sizeof(unsigned) * (size_t)P.sbins;
+    const size_t smem = slots_bytes<SMCRT_R>() + priv_offset(P.sbins) + 8 * (size_t)P.priv_n;
     const bool mods = P.sc.has_mods != 0;
     cudaError_t e;
     if (P.var_tab) {  // second-moment run: the instantiation with the voxel-score tables
@@ -108,6 +108,21 @@ cudaError_t SMCRT_CAT(launch_adjoint, SMCRT_TAG, SMCRT_K)(const Params<SMCRT_R>&
     }
     return cudaGetLastError();
 #endif
+}
+
+// Cells of a privatised fluence sub-box that fit beside the slots and `sbins`
+// shared detector bins in one CTA of the plain kernel on the current device.
+cudaError_t SMCRT_CAT(priv_cells, SMCRT_TAG, SMCRT_K)(int sbins, int* cells) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes a;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, transport_kernel<SMCRT_R, SMCRT_K, false, false, false, false>);
+    if (e != cudaSuccess) return e;
+    const long long room =
+        (long long)optin - (long long)a.sharedSizeBytes - (long long)(slots_bytes<SMCRT_R>() + priv_offset(sbins));
+    *cells = room > 0 ? (int)(room / 8) : 0;
+    return cudaSuccess;
 }
 
 cudaError_t SMCRT_CAT(occupancy, SMCRT_TAG, SMCRT_K)(int block, size_t sbins_bytes, int* per_sm) {

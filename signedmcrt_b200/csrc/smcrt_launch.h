@@ -13,6 +13,7 @@ namespace smcrt {
     cudaError_t launch_##TAG##_##K(const Params<R>& P, const Buffers& B, bool replay, int blocks, int block, \
                                    cudaStream_t s);                                                       \
     cudaError_t occupancy_##TAG##_##K(int block, size_t sbins_bytes, int* per_sm);                   \
+    cudaError_t priv_cells_##TAG##_##K(int sbins, int* cells);                                            \
     cudaError_t launch_batch_##TAG##_##K(const Params<R>& P, const Buffers& B, int blocks, cudaStream_t s);   \
     cudaError_t launch_adjoint_##TAG##_##K(const Params<R>& P, const Buffers& B, int blocks, cudaStream_t s);
 

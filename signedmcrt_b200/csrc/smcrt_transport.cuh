@@ -234,6 +234,27 @@ __device__ __forceinline__ double* tally_grid(const Params<R>& P, int inst) {
     return P.jtab[b & P.tmask];
 }
 
+// Fixed-point unit of the privatised sub-box: 2^-32 cm (a CTA's sum in a voxel stays
+// far below 2^31 cm; a segment's rounding, 1e-10 cm, is below its FP32 rounding).
+constexpr double kPrivScale = 4294967296.0;
+
+// One voxel segment into the fluence tally: the CTA's shared sub-box when the cell
+// lies in it, else the FP64 grid.
+template <class R, bool BATCH>
+__device__ __forceinline__ void tally_add(const Params<R>& P, int inst, int ci, int cj, int ck, int idx, R len,
+                                          unsigned long long* priv) {
+    if (!BATCH && P.priv_n) {
+        const unsigned li = (unsigned)(ci - 1 - P.priv_o[0]), lj = (unsigned)(cj - 1 - P.priv_o[1]),
+                       lk = (unsigned)(ck - 1 - P.priv_o[2]);
+        if (li < (unsigned)P.priv_d[0] && lj < (unsigned)P.priv_d[1] && lk < (unsigned)P.priv_d[2]) {
+            atomicAdd(priv + li + P.priv_d[0] * (lj + P.priv_d[1] * lk),
+                      (unsigned long long)__double2ll_rn((double)len * kPrivScale));
+            return;
+        }
+    }
+    atomicAdd(tally_grid<R, BATCH>(P, inst) + idx, (double)len);
+}
+
 // The scene a kernel instantiation reads: the parameter block's, or (BIG) the
 // device-memory tables of a scene too large for it.
 template <bool BIG, class R>
@@ -577,7 +598,7 @@ __device__ __forceinline__ void var_flush(unsigned char* vt, double* jmean2) {
 // grid the rest of the step, untallied, still counts for survival.)
 template <class R, bool BATCH, bool ADJ, bool VAR>
 __device__ __forceinline__ bool walk_segment(const Params<R>& P, Pk<R>& pk, Flight<R>& f, Cnt& c, float* acc,
-                                             unsigned char* vt) {
+                                             unsigned char* vt, unsigned long long* priv) {
     const GridT<R>& g = P.grid;
     const V3<R>& d = pk.dir;
     const R tm = fmin(f.w.tx, fmin(f.w.ty, f.w.tz));
@@ -585,12 +606,12 @@ __device__ __forceinline__ bool walk_segment(const Params<R>& P, Pk<R>& pk, Flig
     ++c.vox;
     if (tm > f.dsdf) {
         if (ADJ) adj_track(P, pk, acc, (float)(f.dsdf - f.w.td), P.adj_w[idx]);
-        else atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + idx, (double)(f.dsdf - f.w.td));
+        else tally_add<R, BATCH>(P, pk.inst, f.w.ci, f.w.cj, f.w.ck, idx, f.dsdf - f.w.td, priv);
         if (VAR) var_add(vt, P.jmean2, idx, (float)(f.dsdf - f.w.td), c);
         return true;
     }
     if (ADJ) adj_track(P, pk, acc, (float)(tm - f.w.td), P.adj_w[idx]);
-    else atomicAdd(tally_grid<R, BATCH>(P, pk.inst) + idx, (double)(tm - f.w.td));
+    else tally_add<R, BATCH>(P, pk.inst, f.w.ci, f.w.cj, f.w.ck, idx, tm - f.w.td, priv);
     if (VAR) var_add(vt, P.jmean2, idx, (float)(tm - f.w.td), c);
     f.w.td = tm;
     bool out = false;
@@ -730,7 +751,8 @@ __device__ __forceinline__ int step_or_skip(const Params<R>& P, Pk<R>& pk, Fligh
 template <class R, int KERNEL, bool REPLAY, bool BATCH, bool ADJ, bool MODS, bool BIG, bool VAR>
 __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers& B, Pk<R>& pk, Flight<R>& f,
                                                Stream<R, REPLAY>& rng, Cnt& c, int& act, unsigned long long* s_cnt,
-                                               double* s_mom, unsigned* s_bins, float* acc, unsigned char* vt) {
+                                               double* s_mom, unsigned* s_bins, float* acc, unsigned char* vt,
+                                               unsigned long long* priv) {
     const auto& sc = scene_of<BIG>(P);
     const auto& sc64 = scene64_of<BIG>(P);
     using S = std::decay_t<decltype(sc)>;
@@ -1100,7 +1122,7 @@ __device__ __forceinline__ void transport_pass(const Params<R>& P, const Buffers
     // ---- walk voxel segments: at most SMCRT_WALK_SEGMENTS per lane per
     // iteration, so one long walk does not hold up the other lanes' actions
     for (int k = 0; k < SMCRT_WALK_SEGMENTS && act == A_WALK; ++k) {
-        if (walk_segment<R, BATCH, ADJ, VAR>(P, pk, f, c, acc, vt)) {
+        if (walk_segment<R, BATCH, ADJ, VAR>(P, pk, f, c, acc, vt, priv)) {
             pk.pos = advance(pk.pos, f.dsdf, pk.dir);
             cache_move(f);
             if (f.last) {
@@ -1328,6 +1350,9 @@ __device__ __forceinline__ void store_slot(Slots<R, ADJ>& sl, int s, int act, co
     }
 }
 
+// Byte offset of the privatised fluence sub-box after the detector bins (8-aligned).
+__host__ __device__ constexpr size_t priv_offset(int sbins) { return ((size_t)sbins * 4 + 7) / 8 * 8; }
+
 // Dynamic shared memory of one CTA: the slots, then the privatized detector bins.
 template <class R, bool ADJ = false>
 __host__ __device__ constexpr size_t slots_bytes() {
@@ -1361,11 +1386,15 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     extern __shared__ __align__(16) unsigned char s_dyn[];
     Slots<R, ADJ>& sl = *reinterpret_cast<Slots<R, ADJ>*>(s_dyn);
     unsigned* s_bins = reinterpret_cast<unsigned*>(s_dyn + slots_bytes<R, ADJ>());
+    unsigned long long* s_priv =
+        reinterpret_cast<unsigned long long*>(s_dyn + slots_bytes<R, ADJ>() + priv_offset(P.sbins));
     const int t = threadIdx.x;
     const unsigned lane = lane_id();
     if (t < C_NUM) s_cnt[t] = 0ull;
     if (t < 25) s_mom[t] = 0.0;
     for (int i = t; i < P.sbins; i += kBlock) s_bins[i] = 0u;
+    if (!ADJ && !BATCH)
+        for (int i = t; i < P.priv_n; i += kBlock) s_priv[i] = 0ull;
     for (int i = t; i < NS; i += kBlock) sl.meta[i] = (uint32_t)A_NEW;
     // adjoint: per-thread gradient accumulators [3][kMaxAdjGroups][kBlock]
     __shared__ float s_acc[ADJ ? 3 * kMaxAdjGroups * kBlock : 1];
@@ -1470,7 +1499,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
                 for (int r = 0; r < reps; ++r) {
                     transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
                         P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc,
-                        VAR ? vbase + (size_t)s * kVarSlotBytes : nullptr);
+                        VAR ? vbase + (size_t)s * kVarSlotBytes : nullptr, s_priv);
                     if (act == A_DONE) break;
                 }
                 store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
@@ -1494,6 +1523,17 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     if (t < 25 && s_mom[t] != 0.0) atomicAdd(B.moments + t, s_mom[t]);
     for (int i = t; i < P.sbins; i += kBlock)
         if (s_bins[i]) atomicAdd(B.bins + i, (double)s_bins[i]);
+    if (!ADJ && !BATCH && P.priv_n) {  // the privatised sub-box, one FP64 add per nonzero cell
+        double* grid = tally_grid<R, BATCH>(P, 0);
+        for (int i = t; i < P.priv_n; i += kBlock) {
+            const unsigned long long v = s_priv[i];
+            if (!v) continue;
+            const int li = i % P.priv_d[0], lj = (i / P.priv_d[0]) % P.priv_d[1], lk = i / (P.priv_d[0] * P.priv_d[1]);
+            const long long g = (long long)(P.priv_o[0] + li) +
+                                (long long)P.grid.nx * ((P.priv_o[1] + lj) + (long long)P.grid.ny * (P.priv_o[2] + lk));
+            atomicAdd(grid + g, (double)(long long)v / kPrivScale);
+        }
+    }
     if (ADJ && t < 3 * P.adj_ngroups) {  // thread (k, group) sums its row over the CTA's threads
         const int k = t / P.adj_ngroups, grp = t % P.adj_ngroups;
         const float* row = s_acc + (k * kMaxAdjGroups + grp) * kBlock;

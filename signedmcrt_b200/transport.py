@@ -38,7 +38,7 @@ class Transport:
                  end_early: bool = False, stream: int | None = None, block_size: int = 0, blocks_per_sm: int = 0,
                  eps: float = 0.0, normal_h: float = 0.0, max_trace_steps: int = 0, timeout_ms: int = 0,
                  instance: int = 0, tally_copies: int = 0, scene_memory: int = 0, variance: bool = False,
-                 nearest_cache: int = 0):
+                 nearest_cache: int = 0, shared_fluence: int = 0):
         self.settings = settings
         self.flat = array if isinstance(array, FlatScene) else FlatScene(array)
         self.grid = settings.grid_c()
@@ -59,6 +59,7 @@ class Transport:
         o.scene_memory = scene_memory  # 1: the scene from device memory even when it fits the parameter block
         o.variance = int(bool(variance))  # keep the per-voxel second moment (run_moments)
         o.nearest_cache = nearest_cache  # 0: library choice; 1: on where allowed; 2: off
+        o.shared_fluence = shared_fluence  # 0: library choice (autotuned); 1: on (FP32 pencil); 2: off
         # stream=None: a stream private to this context; an int: that cudaStream_t (0 = default)
         o.stream = stream if stream is not None else None
         o.private_stream = int(stream is None)
@@ -154,7 +155,7 @@ class Transport:
         return {"tally_copies": t.tally_copies, "shared_bins": bool(t.shared_bins),
                 "packets_per_s": t.packets_per_s, "trials": t.trials, "block_size": t.block_size,
                 "slots_per_thread": t.slots_per_thread, "ctas_per_sm": t.ctas_per_sm,
-                "nearest_cache": bool(t.nearest_cache)}
+                "nearest_cache": bool(t.nearest_cache), "shared_fluence": bool(t.shared_fluence)}
 
     def run_device(self, first: int, count: int, seed: int, jmean_dev: int, bins_dev: int | None,
                    stats: bool = False) -> dict | None:

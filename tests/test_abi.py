@@ -63,7 +63,7 @@ STRUCTS = {
     "smcrt_options": (abi.Options, ["kernel", "precision", "end_early", "block_size", "blocks_per_sm",
                                     "max_trace_steps", "eps", "normal_h", "instance", "timeout_ms", "stream",
                                     "private_stream", "tally_copies", "scene_memory", "variance", "nearest_cache",
-                                    "reserved"]),
+                                    "shared_fluence", "reserved"]),
     "smcrt_stats": (abi.Stats, ["nscatt", "packets", "sdf_evals", "voxel_segments", "trace_steps", "scatters",
                                 "fresnel_events", "reflections", "kills_step_cap", "kills_error", "rng_draws",
                                 "moments", "kernel_ms", "device_status", "h2d_bytes", "d2h_bytes",
@@ -71,7 +71,8 @@ STRUCTS = {
     "smcrt_packet_state": (abi.PacketState, ["pos", "dir", "weight", "layer", "nscatt", "ndraws", "flags"]),
     "smcrt_region_optics": (abi.RegionOptics, ["mus", "mua", "hgg", "n"]),
     "smcrt_tuning": (abi.Tuning, ["tally_copies", "shared_bins", "packets_per_s", "trials", "block_size",
-                                  "slots_per_thread", "ctas_per_sm", "nearest_cache"]),
+                                  "slots_per_thread", "ctas_per_sm", "nearest_cache",
+                                  "shared_fluence"]),
 }
 
 
