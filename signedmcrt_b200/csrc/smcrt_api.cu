@@ -104,6 +104,11 @@ void fill_grid(GridT<R>& g, const smcrt_grid& s) {
     g.sx_d = (double)s.nxg / (2.0 * s.xmax);
     g.sy_d = (double)s.nyg / (2.0 * s.ymax);
     g.sz_d = (double)s.nzg / (2.0 * s.zmax);
+    // the same expression as the walk's face positions had on the device (2.0 * max / n,
+    // IEEE-rounded), computed once here instead of three FP64 divisions a step
+    g.vx_d = 2.0 * s.xmax / (double)s.nxg;
+    g.vy_d = 2.0 * s.ymax / (double)s.nyg;
+    g.vz_d = 2.0 * s.zmax / (double)s.nzg;
 }
 
 template <class R>

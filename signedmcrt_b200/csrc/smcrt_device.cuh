@@ -500,6 +500,7 @@ struct GridT {
     R sx, sy, sz;       // n/(2*max) as written: n * p / (2 * max)
     double xmax_d, ymax_d, zmax_d;  // exact half sizes (grid-exit test on FP64 positions)
     double sx_d, sy_d, sz_d;        // n / (2 max) in FP64 (FP32 transport's cell index of an FP64 position)
+    double vx_d, vy_d, vz_d;        // voxel sizes 2 max / n in FP64 (the walk's face positions)
 };
 
 struct DetT {
