@@ -1170,23 +1170,6 @@ constexpr int kGroups = 5;
 #ifndef SMCRT_DRAIN_PASSES
 #define SMCRT_DRAIN_PASSES 16
 #endif
-// Chunks a warp of the queue scheduler takes between two reads of the time
-// budget's clock.
-constexpr unsigned kBudgetPops = 64;
-// Scheduler: work queues per sort group (1) or counting-sort rounds (0).
-// Adjoint launches always use the rounds (their accumulators leave no shared
-// memory for the rings).
-#ifndef SMCRT_QUEUE
-#define SMCRT_QUEUE 0
-#endif
-constexpr bool kQueueSched = SMCRT_QUEUE != 0;
-// Ring entries: slot index | valid bit; a ring is a power of two >= the slots.
-constexpr unsigned kRingValid = 0x8000u;
-template <int N>
-constexpr int kRingSize = N <= 512 ? 512 : N <= 1024 ? 1024 : N <= 2048 ? 2048 : 4096;
-// Polls of an empty queue or of an unwritten entry before the CTA gives up
-// (STATUS_ABORTED): far beyond any pass's length.
-constexpr unsigned kIdleLimit = 1u << 24;
 constexpr int kDrainLive = SMCRT_DRAIN_LIVE_PER_WARP * (kBlock / 32);
 constexpr int kDrainPasses = SMCRT_DRAIN_PASSES;
 static_assert(SMCRT_DRAIN_LIVE_PER_WARP <= 32, "one drain item per lane at most");
@@ -1428,157 +1411,15 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
     // this CTA's voxel-score tables (second-moment runs)
     unsigned char* const vbase = VAR ? P.var_tab + (size_t)blockIdx.x * NS * kVarSlotBytes : nullptr;
     const unsigned lt = (1u << lane) - 1u;
-    constexpr int NW = kBlock / 32;
-    const int warp = t >> 5;
-    if constexpr (kQueueSched && !ADJ) {
-    // ---- work queues: one ring of slot indices per sort group.  A warp pops up
-    // to 32 slots of one group (the first group, in list order, holding a full
-    // chunk, else the fullest), runs one pass of each, and pushes every packet
-    // onto the ring of its next action's group.  No CTA barrier: a warp that is
-    // done takes the next chunk at once, whatever the other warps are doing.
-    // Entries carry a valid bit: a pusher reserves positions first (s_resv) and
-    // writes them after, a popper reserves a range of written-or-soon-written
-    // positions (CAS on s_head) and waits for each entry's bit (bounded).
-    constexpr int RING = kRingSize<NS>;
-    __shared__ unsigned short s_ring[kGroups][RING];
-    __shared__ unsigned s_head[kGroups], s_resv[kGroups];
-    __shared__ int s_ndone, s_qstop;
-    for (int i = t; i < kGroups * RING; i += kBlock) (&s_ring[0][0])[i] = 0;
-    __syncthreads();
-    for (int i = t; i < NS; i += kBlock) s_ring[act_group(A_NEW)][i] = (unsigned short)(i | kRingValid);
-    if (t < kGroups) {
-        s_head[t] = 0u;
-        s_resv[t] = t == act_group(A_NEW) ? (unsigned)NS : 0u;
-    }
-    if (t == 0) {
-        s_ndone = 0;
-        s_qstop = 0;
-    }
-    __syncthreads();
-    volatile unsigned* vhead = s_head;
-    volatile unsigned* vresv = s_resv;
-    volatile int* vndone = &s_ndone;
-    volatile int* vstop = &s_qstop;
-    volatile unsigned short* vring = &s_ring[0][0];
-    unsigned idle = 0;
-    for (unsigned pops = 0;; ++pops) {
-        int pg = -1, pn = 0, stop = 0, finished = 0;
-        unsigned ph = 0;
-        int live = NS;
-        if (lane == 0) {
-            if (P.budget_ns && (pops % kBudgetPops) == 0 && global_ns() - t0 > P.budget_ns) {
-                atomicOr(B.status, STATUS_ABORTED);
-                *vstop = 1;
-            }
-            live = NS - *vndone;
-            // few live packets: a few per warp, each run for kDrainPasses passes
-            const int cap = live <= kDrainLive ? max(1, (live + NW - 1) / NW) : 32;
-            for (int attempt = 0; attempt < 4 && !*vstop; ++attempt) {
-                int best = -1, bav = 0;
-#pragma unroll
-                for (int g = 0; g < kGroups; ++g) {
-                    const int av = (int)(vresv[g] - vhead[g]);
-                    if (av >= cap) {
-                        best = g;
-                        bav = av;
-                        break;
-                    }
-                    if (av > bav) {
-                        best = g;
-                        bav = av;
-                    }
-                }
-                if (best < 0) break;
-                const unsigned h = vhead[best];
-                const int n = min(cap, (int)(vresv[best] - h));
-                if (n <= 0) continue;
-                if (atomicCAS(&s_head[best], h, h + (unsigned)n) == h) {
-                    pg = best;
-                    pn = n;
-                    ph = h;
-                    break;
-                }
-            }
-            stop = *vstop;
-            finished = *vndone >= NS;
-        }
-        // lane 0's view, so that the warp decides as one
-        pg = __shfl_sync(0xffffffffu, pg, 0);
-        pn = __shfl_sync(0xffffffffu, pn, 0);
-        ph = __shfl_sync(0xffffffffu, ph, 0);
-        live = __shfl_sync(0xffffffffu, live, 0);
-        stop = __shfl_sync(0xffffffffu, stop, 0);
-        finished = __shfl_sync(0xffffffffu, finished, 0);
-        if (stop && pn == 0) break;
-        if (pn == 0) {
-            if (finished) break;  // every slot has retired for good
-            // nothing poppable now: other warps hold the live packets
-            if (++idle > kIdleLimit) {
-                if (lane == 0) {
-                    atomicOr(B.status, STATUS_ABORTED);
-                    *vstop = 1;
-                }
-                break;
-            }
-            __nanosleep(64);
-            continue;
-        }
-        idle = 0;
-        int s = -1;
-        if ((int)lane < pn) {
-            volatile unsigned short* e = vring + pg * RING + ((ph + lane) & (RING - 1));
-            unsigned v = *e;
-            for (unsigned w = 0; !(v & kRingValid) && w < kIdleLimit; ++w) v = *e;
-            if (v & kRingValid) {
-                s = (int)(v & (kRingValid - 1u));
-                *e = 0;
-            } else {
-                atomicOr(B.status, STATUS_ABORTED);
-                *vstop = 1;
-            }
-        }
-        __threadfence_block();  // the slots' states, written before their entries
-        const int reps = live <= kDrainLive ? kDrainPasses : 1;
-        int act = A_DONE;
-        if (s >= 0) {
-            act = load_slot<R, REPLAY, BATCH, ADJ>(sl, s, P, B, pk, f, rng);
-            for (int r = 0; r < reps; ++r) {
-                transport_pass<R, KERNEL, REPLAY, BATCH, ADJ, MODS, BIG, VAR>(
-                    P, B, pk, f, rng, c, act, s_cnt, s_mom, s_bins, s_acc,
-                    VAR ? vbase + (size_t)s * kVarSlotBytes : nullptr, s_priv);
-                if (act == A_DONE) break;
-            }
-            store_slot<R, REPLAY, BATCH, ADJ>(sl, s, act, pk, f, rng);
-        }
-        __threadfence_block();  // the slots' states before their ring entries
-        // push: lanes with the same next group share one reservation
-        const int key = s < 0 ? kGroups + 1 : act == A_DONE ? kGroups : act_group(act);
-        const unsigned m = __match_any_sync(0xffffffffu, key);
-        const int leader = __ffs(m) - 1;
-        unsigned base = 0;
-        if ((int)lane == leader) {
-            if (key < kGroups) base = atomicAdd(&s_resv[key], (unsigned)__popc(m));
-            else if (key == kGroups) atomicAdd(&s_ndone, __popc(m));
-        }
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (key < kGroups) {
-            volatile unsigned short* e = vring + key * RING + ((base + (unsigned)__popc(m & lt)) & (RING - 1));
-            // the position's previous entry has been read (it always has: a ring
-            // holds at most NS < RING entries); bounded all the same
-            for (unsigned w = 0; (*e & kRingValid) && w < kIdleLimit; ++w) {
-            }
-            *e = (unsigned short)(s | kRingValid);
-        }
-    }
-    __syncthreads();
-    } else {
     // ---- rounds: each round counting-sorts the live slots by action (warp
     // ballots and a per-warp scan, stable in slot order) and the warps take
     // 32-item chunks of the sorted list; three CTA barriers a round
     constexpr int Q = SlotCount<R>::per_thread;
+    constexpr int NW = kBlock / 32;
     __shared__ int s_off[kGroups][Q][NW];
     __shared__ unsigned short s_list[NS];
     __shared__ int s_next;
+    const int warp = t >> 5;
     for (;;) {
         __syncthreads();  // the previous round's slot writes are visible
         int a[Q], rank[Q];
@@ -1668,7 +1509,6 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
             if (lane == 0) next = atomicAdd(&s_next, 1);
             chunk = __shfl_sync(0xffffffffu, next, 0);
         }
-    }
     }
     // events of packets still in flight (time budget) and since the last retire
     atomicAdd(&s_cnt[C_SDF], (unsigned long long)c.sdf);
