@@ -501,6 +501,12 @@ def main() -> None:
                     help="nearest-region sweep cache: 0 library choice, 1 on, 2 off")
     ap.add_argument("--shared-fluence", type=int, default=0, choices=(0, 1, 2),
                     help="shared-memory beam sub-box of the fluence (FP32 pencil beams): 0 library choice, 1 on, 2 off")
+    ap.add_argument("--group-order", type=int, default=0, choices=(0, 1, 2),
+                    help="order of the action groups in the kernel's per-round packet list: 0 library choice "
+                         "(walk chunks last), 1 walk last, 2 interactions last")
+    ap.add_argument("--tune-packets", type=float, default=2e6,
+                    help="packets of each smcrt_autotune trial run before the timed region (box_slab, "
+                         "sphere_water, layered_vessels; skipped when an option above is given explicitly); 0: off")
     ap.add_argument("--num-spheres", type=int, default=40,
                     help="sphere_scene: spheres of the reference's res/sphere.toml scene (regions = this + 1)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample length")
@@ -563,7 +569,21 @@ def main() -> None:
     stream = torch.cuda.Stream(dev)  # every timed launch goes to this stream
     torch.cuda.set_stream(stream)
     tr = T.Transport(flat, st, precision=args.precision, stream=stream.cuda_stream, timeout_ms=600000,
-                     eps=args.eps, nearest_cache=args.nearest_cache, shared_fluence=args.shared_fluence)
+                     eps=args.eps, nearest_cache=args.nearest_cache, shared_fluence=args.shared_fluence,
+                     group_order=args.group_order)
+    # the library's autotuner picks the launch configuration (fluence-grid copies,
+    # detector-bin privatisation, nearest-region cache, shared fluence sub-box, group
+    # order) from timed trial runs, outside the timed region; the e2e context below
+    # is made with the same choices (its detector bins: the library's default)
+    tuning = None
+    if (args.tune_packets > 0 and args.config in ("box_slab", "sphere_water", "layered_vessels")
+            and not (args.group_order or args.nearest_cache or args.shared_fluence)):
+        tuning = tr.autotune(int(min(per_gpu, args.tune_packets)), 12345)
+    host_opts = dict(nearest_cache=args.nearest_cache, shared_fluence=args.shared_fluence,
+                     group_order=args.group_order)
+    if tuning is not None:
+        host_opts = dict(tally_copies=tuning["tally_copies"], nearest_cache=1 if tuning["nearest_cache"] else 2,
+                         shared_fluence=1 if tuning["shared_fluence"] else 2, group_order=tuning["group_order"])
     jm = torch.zeros(tr.ncell, dtype=torch.float64, device=dev)
     bins = torch.zeros(max(tr.nbins, 1), dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
@@ -618,8 +638,7 @@ def main() -> None:
     if not args.no_e2e:
         jh = torch.empty(tr.ncell, dtype=torch.float64, pin_memory=True).numpy()
         bh = torch.empty(max(tr.nbins, 1), dtype=torch.float64, pin_memory=True).numpy()
-        tr_host = T.Transport(flat, st, precision=args.precision, timeout_ms=600000, eps=args.eps,
-                              nearest_cache=args.nearest_cache, shared_fluence=args.shared_fluence)
+        tr_host = T.Transport(flat, st, precision=args.precision, timeout_ms=600000, eps=args.eps, **host_opts)
         tr_host.run(min(per_gpu, 100000), 1, jmean_out=jh, bins_out=bh[:tr_host.nbins] if tr_host.nbins else None)
         if world > 1:
             dist.barrier()
@@ -672,6 +691,10 @@ def main() -> None:
             "gpu_launches": args.steps,
             "clocks": clocks,
         }
+        if tuning is not None:
+            line["tuning"] = {k: tuning[k] for k in ("tally_copies", "shared_bins", "nearest_cache",
+                                                     "shared_fluence", "group_order", "trials")}
+            line["tuning"]["trial_packets"] = int(min(per_gpu, args.tune_packets))
         if e2e is not None:
             line["e2e"] = e2e
         if world == 1 and not args.no_cpu_baseline:

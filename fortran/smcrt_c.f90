@@ -20,7 +20,7 @@ module smcrt_c
     implicit none
     private :: c_strlen
 
-    integer(c_int32_t), parameter :: SMCRT_ABI_VERSION_EXPECTED = 4
+    integer(c_int32_t), parameter :: SMCRT_ABI_VERSION_EXPECTED = 5
 
     ! smcrt_status
     integer(c_int32_t), parameter :: SMCRT_OK = 0, SMCRT_ERR_ARG = 1, SMCRT_ERR_SCENE = 2, SMCRT_ERR_CUDA = 3, &
@@ -45,6 +45,7 @@ module smcrt_c
     ! smcrt_kernel_kind, smcrt_precision
     integer(c_int32_t), parameter :: SMCRT_KERNEL_PATHLENGTH = 0, SMCRT_KERNEL_WEIGHT = 1, SMCRT_KERNEL_TEST = 2
     integer(c_int32_t), parameter :: SMCRT_FP32 = 0, SMCRT_FP64 = 1
+    integer(c_int32_t), parameter :: SMCRT_ORDER_WALK_LAST = 1, SMCRT_ORDER_INTERACT_LAST = 2
 
     type, bind(C) :: smcrt_prim
         integer(c_int32_t) :: kind, nmods
@@ -86,7 +87,7 @@ module smcrt_c
         integer(c_int32_t) :: instance, timeout_ms
         type(c_ptr)        :: stream
         integer(c_int32_t) :: private_stream, tally_copies, scene_memory, variance, nearest_cache
-        integer(c_int32_t) :: shared_fluence, reserved(4)
+        integer(c_int32_t) :: shared_fluence, group_order, reserved(3)
     end type smcrt_options
 
     type, bind(C) :: smcrt_stats
@@ -107,6 +108,7 @@ module smcrt_c
         integer(c_int32_t) :: tally_copies, shared_bins
         real(c_double)     :: packets_per_s
         integer(c_int32_t) :: trials, block_size, slots_per_thread, ctas_per_sm, nearest_cache, shared_fluence
+        integer(c_int32_t) :: group_order, reserved
     end type smcrt_tuning
 
     type, bind(C) :: smcrt_region_optics

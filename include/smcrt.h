@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define SMCRT_ABI_VERSION 4
+#define SMCRT_ABI_VERSION 5
 
 /* ---- status codes -------------------------------------------------------- */
 enum smcrt_status {
@@ -173,6 +173,14 @@ enum smcrt_kernel_kind {
     SMCRT_KERNEL_TEST = 2        /* test_kernel: scatter-order position moments */
 };
 enum smcrt_precision { SMCRT_FP32 = 0, SMCRT_FP64 = 1 };
+/* Order of the action groups in the transport kernel's per-round sorted packet
+ * list (smcrt_options.group_order).  The FP64 near-surface sweeps come first and
+ * the sweeps second in both; the warps take chunks of the list from its head, so
+ * the last group's chunks end each round.  The order changes only the speed. */
+enum smcrt_group_order {
+    SMCRT_ORDER_WALK_LAST = 1,     /* ..., interactions, voxel walks, launches */
+    SMCRT_ORDER_INTERACT_LAST = 2  /* ..., voxel walks, interactions, launches */
+};
 
 typedef struct smcrt_options {
     int32_t kernel;        /* smcrt_kernel_kind */
@@ -219,7 +227,12 @@ typedef struct smcrt_options {
                               as 64-bit fixed point (2^-32 cm) and adds it to the FP64
                               grid once; 0 = library choice (off unless smcrt_autotune
                               picks it), 1 = on, 2 = off */
-    int32_t reserved[4];   /* zero */
+    int32_t group_order;   /* order of the action groups in each round's sorted list of
+                              packets (the warps take its chunks from the head; no
+                              counterpart in the reference, results unchanged):
+                              0 = library choice (SMCRT_ORDER_WALK_LAST unless
+                              smcrt_autotune picks the other), or one of smcrt_group_order */
+    int32_t reserved[3];   /* zero */
 } smcrt_options;
 
 /* Event counters of one run (definitions identical in the CPU oracle). */
@@ -319,6 +332,8 @@ typedef struct smcrt_tuning {
     int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent grid */
     int32_t nearest_cache; /* 1: sweeps skip regions the nearest-region cache rules out */
     int32_t shared_fluence; /* 1: each CTA sums a beam-axis sub-box of the fluence in shared memory */
+    int32_t group_order;   /* chosen smcrt_group_order */
+    int32_t reserved;      /* zero */
 } smcrt_tuning;
 int32_t smcrt_autotune(smcrt_ctx* ctx, int64_t trial_packets, uint64_t seed, smcrt_tuning* result);
 

@@ -8,7 +8,7 @@ import ctypes as C
 
 import numpy as np
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 # status
 OK, ERR_ARG, ERR_SCENE, ERR_CUDA, ERR_DEVICE, ERR_TIMEOUT, ERR_NO_DEVICE = range(7)
@@ -25,6 +25,8 @@ DET_CIRCLE, DET_ANNULUS, DET_CAMERA = 1, 2, 3
 # kernels / precision
 KERNEL_PATHLENGTH, KERNEL_WEIGHT, KERNEL_TEST = 0, 1, 2
 FP32, FP64 = 0, 1
+# order of the action groups in the kernel's per-round packet list (options.group_order)
+ORDER_WALK_LAST, ORDER_INTERACT_LAST = 1, 2
 
 D3 = C.c_double * 3
 
@@ -69,7 +71,8 @@ class Options(C.Structure):
                 ("eps", C.c_double), ("normal_h", C.c_double), ("instance", C.c_uint32),
                 ("timeout_ms", C.c_int32), ("stream", C.c_void_p), ("private_stream", C.c_int32),
                 ("tally_copies", C.c_int32), ("scene_memory", C.c_int32), ("variance", C.c_int32),
-                ("nearest_cache", C.c_int32), ("shared_fluence", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("nearest_cache", C.c_int32), ("shared_fluence", C.c_int32), ("group_order", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class Stats(C.Structure):
@@ -133,7 +136,8 @@ class RegionOptics(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("tally_copies", C.c_int32), ("shared_bins", C.c_int32), ("packets_per_s", C.c_double),
                 ("trials", C.c_int32), ("block_size", C.c_int32), ("slots_per_thread", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("nearest_cache", C.c_int32), ("shared_fluence", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("nearest_cache", C.c_int32), ("shared_fluence", C.c_int32),
+                ("group_order", C.c_int32), ("reserved", C.c_int32)]
 
 
 # Exported symbols of include/smcrt.h with their argtypes/restype.

@@ -217,10 +217,18 @@ double near_band(double eps, const smcrt_grid& g) {
 // The per-flight sphere-trace step count shares its slot word with the
 // nearest-region cache: 21 bits.
 constexpr int kMaxTraceSteps = (1 << 21) - 1;
+// Option checks shared by contexts, batches and the allocation-free run.
 int check_steps(const smcrt_options* o) {
     if (o && o->max_trace_steps > kMaxTraceSteps)
         return fail(SMCRT_ERR_ARG, "options: max_trace_steps must be at most " + std::to_string(kMaxTraceSteps));
+    if (o && (o->group_order < 0 || o->group_order > SMCRT_ORDER_INTERACT_LAST))
+        return fail(SMCRT_ERR_ARG, "options: group_order must be 0, 1 or 2");
     return SMCRT_OK;
+}
+
+// The kernel's nibble table for an smcrt_group_order (0: the library's choice).
+unsigned group_order_table(int order) {
+    return order == SMCRT_ORDER_INTERACT_LAST ? kOrderInteractLast : kOrderWalkLast;
 }
 
 int pick_device(int& dev, int& nsm) {
@@ -368,6 +376,7 @@ void fill_params(Params<R>* P, const smcrt_scene* scene, const smcrt_grid* grid,
     const bool allowed = cache_policy(scene, grid, (int)sizeof(R), &P->cache_margin);
     const int want = o ? o->nearest_cache : 0;
     P->cache_ok = allowed && want != 2 ? 1 : 0;
+    P->group_order = group_order_table(o ? o->group_order : 0);
     P->normal_h = (o && o->normal_h > 0) ? o->normal_h : 1e-6;
     P->instance = o ? o->instance : 0u;
     P->tcopies = 1;
@@ -875,7 +884,8 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
     g_err.clear();
     if (!c || trial_packets < 1) return fail(SMCRT_ERR_ARG, "autotune: bad arguments");
     // candidates: fluence-grid copies 1, 2, 4, 8 (as many as fit in 256 MiB), detector bins
-    // in shared memory or not (only when there are bins that fit)
+    // in shared memory or not (only when there are bins that fit), the nearest-region
+    // cache and the shared fluence sub-box where allowed, and both group orders
     std::vector<int> copies;
     for (int k = 1; k <= 8; k *= 2)
         if (k == 1 || (long long)k * c->ncell * 8 <= (256ll << 20)) copies.push_back(k);
@@ -895,6 +905,11 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
     if (c->cache_allowed) caches.push_back(1);
     std::vector<int> privs = {0};
     if (c->priv_allowed) privs.push_back(1);
+    const std::vector<int> orders = {SMCRT_ORDER_WALK_LAST, SMCRT_ORDER_INTERACT_LAST};
+    auto set_order = [&](int order) {
+        if (c->pf) c->pf->group_order = group_order_table(order);
+        if (c->pd) c->pd->group_order = group_order_table(order);
+    };
     const int keep_tc = c->tcopies;
     const bool keep_sb = c->shared_bins_on;
     auto set_cache = [&](int on) {
@@ -904,14 +919,18 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
     double best = -1.0;
     int best_tc = keep_tc, best_sb = keep_sb, best_cache = c->pf ? c->pf->cache_ok : c->pd->cache_ok, trials = 0;
     int best_priv = c->priv_on;
+    const unsigned keep_order = c->pf ? c->pf->group_order : c->pd->group_order;
+    int best_order = keep_order == kOrderInteractLast ? SMCRT_ORDER_INTERACT_LAST : SMCRT_ORDER_WALK_LAST;
     for (int tc : copies)
         for (int sb : sbins)
           for (int ca : caches)
-            for (int pv : privs) {
+            for (int pv : privs)
+              for (int go : orders) {
             c->tcopies = tc;
             c->shared_bins_on = sb != 0;
             set_cache(ca);
             c->priv_on = pv != 0;
+            set_order(go);
             double best_here = 0.0;
             for (int rep = 0; rep < 2; ++rep) {  // best of two: the first may pay cold caches
                 CK(cudaMemsetAsync(c->d_jmean, 0, sizeof(double) * c->ncell, c->stream));
@@ -933,12 +952,14 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
                 best_sb = sb;
                 best_cache = ca;
                 best_priv = pv;
+                best_order = go;
             }
         }
     c->tcopies = best_tc;
     c->shared_bins_on = best_sb != 0;
     set_cache(best_cache);
     c->priv_on = best_priv != 0;
+    set_order(best_order);
     if (result) {
         result->tally_copies = best_tc;
         result->shared_bins = best_sb;
@@ -950,6 +971,8 @@ int32_t smcrt_autotune(smcrt_ctx* c, int64_t trial_packets, uint64_t seed, smcrt
         result->ctas_per_sm = c->grid_blocks / std::max(1, c->nsm);
         result->nearest_cache = best_cache;
         result->shared_fluence = best_priv;
+        result->group_order = best_order;
+        result->reserved = 0;
     }
     return SMCRT_OK;
 }

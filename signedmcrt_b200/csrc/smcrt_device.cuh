@@ -541,6 +541,8 @@ struct Params {
     // margin of its test (FP32 transport: the FP32 sweeps' margin for both sweeps)
     int cache_ok;
     double cache_margin;
+    // sort group of each action, one nibble per action (the round's list order)
+    unsigned group_order;
     // shared-memory fluence privatisation (FP32 plain launches): a sub-box of
     // voxels (0-based origin, extents; priv_n cells, 0 = off) whose segments each
     // CTA sums in shared memory as 64-bit fixed point and adds to the grid once

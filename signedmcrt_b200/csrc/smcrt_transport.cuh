@@ -1153,14 +1153,15 @@ struct SlotCount {
     static constexpr int n = kBlock * per_thread;
 };
 // Sort groups of the actions a packet can wait in between rounds, in list
-// order: FP64 near-surface sweep, sweep (or a pending crossing), walk, interact,
-// retire/launch.  Each warp's first chunk is fixed (warp w, chunk w), so the
-// costly FP64 chunks at the head of the list go to different warps; the rest of
-// the list goes to whichever warp finishes first.  A_DONE maps to kGroups (not
-// listed).  Nibble `act` of SMCRT_GROUP_ORDER is the group of action `act`.
-#ifndef SMCRT_GROUP_ORDER
-#define SMCRT_GROUP_ORDER 0x05431214u
-#endif
+// order: FP64 near-surface sweep, sweep (or a pending crossing), then walk,
+// interact and retire/launch in the order of the launch's group_order.  Each
+// warp's first chunk is fixed (warp w, chunk w), so the costly FP64 chunks at
+// the head of the list go to different warps; the rest of the list goes to
+// whichever warp finishes first, so the last group's chunks end each round.
+// A_DONE maps to kGroups (not listed).  Nibble `act` of an order is the group
+// of action `act`.
+constexpr unsigned kOrderWalkLast = 0x05421314u;      // sweep, interact, walk, launch
+constexpr unsigned kOrderInteractLast = 0x05431214u;  // sweep, walk, interact, launch
 constexpr int kGroups = 5;
 // Drain mode: at most this many live slots in a CTA (a few per warp), each run
 // for kDrainPasses passes per round.
@@ -1173,7 +1174,7 @@ constexpr int kGroups = 5;
 constexpr int kDrainLive = SMCRT_DRAIN_LIVE_PER_WARP * (kBlock / 32);
 constexpr int kDrainPasses = SMCRT_DRAIN_PASSES;
 static_assert(SMCRT_DRAIN_LIVE_PER_WARP <= 32, "one drain item per lane at most");
-__device__ __forceinline__ int act_group(int act) { return (int)((SMCRT_GROUP_ORDER >> (4 * act)) & 0xFu); }
+__device__ __forceinline__ int act_group(unsigned order, int act) { return (int)((order >> (4 * act)) & 0xFu); }
 template <class R, bool ADJ, int kSlots = SlotCount<R>::n>
 struct Slots {
     static constexpr int kRW = sizeof(R) / 4;  // 32-bit words per R
@@ -1425,7 +1426,7 @@ __global__ void __launch_bounds__(kBlock, SMCRT_MIN_BLOCKS) transport_kernel(con
         int a[Q], rank[Q];
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            a[q] = act_group((int)(sl.meta[t + q * kBlock] & 7u));
+            a[q] = act_group(P.group_order, (int)(sl.meta[t + q * kBlock] & 7u));
             rank[q] = 0;
 #pragma unroll
             for (int g = 0; g < kGroups; ++g) {

@@ -38,7 +38,7 @@ class Transport:
                  end_early: bool = False, stream: int | None = None, block_size: int = 0, blocks_per_sm: int = 0,
                  eps: float = 0.0, normal_h: float = 0.0, max_trace_steps: int = 0, timeout_ms: int = 0,
                  instance: int = 0, tally_copies: int = 0, scene_memory: int = 0, variance: bool = False,
-                 nearest_cache: int = 0, shared_fluence: int = 0):
+                 nearest_cache: int = 0, shared_fluence: int = 0, group_order: int = 0):
         self.settings = settings
         self.flat = array if isinstance(array, FlatScene) else FlatScene(array)
         self.grid = settings.grid_c()
@@ -60,6 +60,7 @@ class Transport:
         o.variance = int(bool(variance))  # keep the per-voxel second moment (run_moments)
         o.nearest_cache = nearest_cache  # 0: library choice; 1: on where allowed; 2: off
         o.shared_fluence = shared_fluence  # 0: library choice (autotuned); 1: on (FP32 pencil); 2: off
+        o.group_order = group_order  # 0: library choice; abi.ORDER_WALK_LAST / abi.ORDER_INTERACT_LAST
         # stream=None: a stream private to this context; an int: that cudaStream_t (0 = default)
         o.stream = stream if stream is not None else None
         o.private_stream = int(stream is None)
@@ -149,13 +150,15 @@ class Transport:
 
     def autotune(self, trial_packets: int = 200000, seed: int = 0) -> dict:
         """smcrt_autotune: times trial runs of each launch configuration (fluence-grid
-        copies, detector-bin privatisation) and keeps the fastest for later runs."""
+        copies, detector-bin privatisation, the nearest-region cache, the shared
+        fluence sub-box, the group order) and keeps the fastest for later runs."""
         t = abi.Tuning()
         check(lib().smcrt_autotune(self._ctx, int(trial_packets), int(seed), C.byref(t)))
         return {"tally_copies": t.tally_copies, "shared_bins": bool(t.shared_bins),
                 "packets_per_s": t.packets_per_s, "trials": t.trials, "block_size": t.block_size,
                 "slots_per_thread": t.slots_per_thread, "ctas_per_sm": t.ctas_per_sm,
-                "nearest_cache": bool(t.nearest_cache), "shared_fluence": bool(t.shared_fluence)}
+                "nearest_cache": bool(t.nearest_cache), "shared_fluence": bool(t.shared_fluence),
+                "group_order": int(t.group_order)}
 
     def run_device(self, first: int, count: int, seed: int, jmean_dev: int, bins_dev: int | None,
                    stats: bool = False) -> dict | None:

@@ -63,7 +63,7 @@ STRUCTS = {
     "smcrt_options": (abi.Options, ["kernel", "precision", "end_early", "block_size", "blocks_per_sm",
                                     "max_trace_steps", "eps", "normal_h", "instance", "timeout_ms", "stream",
                                     "private_stream", "tally_copies", "scene_memory", "variance", "nearest_cache",
-                                    "shared_fluence", "reserved"]),
+                                    "shared_fluence", "group_order", "reserved"]),
     "smcrt_stats": (abi.Stats, ["nscatt", "packets", "sdf_evals", "voxel_segments", "trace_steps", "scatters",
                                 "fresnel_events", "reflections", "kills_step_cap", "kills_error", "rng_draws",
                                 "moments", "kernel_ms", "device_status", "h2d_bytes", "d2h_bytes",
@@ -72,7 +72,7 @@ STRUCTS = {
     "smcrt_region_optics": (abi.RegionOptics, ["mus", "mua", "hgg", "n"]),
     "smcrt_tuning": (abi.Tuning, ["tally_copies", "shared_bins", "packets_per_s", "trials", "block_size",
                                   "slots_per_thread", "ctas_per_sm", "nearest_cache",
-                                  "shared_fluence"]),
+                                  "shared_fluence", "group_order", "reserved"]),
 }
 
 
@@ -117,6 +117,19 @@ def test_render_checks_its_arguments_before_the_device():
         with pytest.raises(_lib.SmcrtError) as e:
             T.render(arr, (4, 4, 4), (1.0, 1.0, 1.0))
         assert e.value.code == abi.ERR_NO_DEVICE
+
+
+def test_group_order_is_checked_before_the_device():
+    """options.group_order takes 0 (library choice), SMCRT_ORDER_WALK_LAST or
+    SMCRT_ORDER_INTERACT_LAST; anything else is SMCRT_ERR_ARG before any device
+    is touched."""
+    from signedmcrt_b200 import _lib, presets as P, transport as T
+    st = P.benchmark_settings("box_slab")
+    for bad in (-1, 3):
+        with pytest.raises(_lib.SmcrtError) as e:
+            T.Transport(P.setup_simulation(st), st, group_order=bad)
+        assert e.value.code == abi.ERR_ARG
+    assert (abi.ORDER_WALK_LAST, abi.ORDER_INTERACT_LAST) == (1, 2)
 
 
 def test_trace_step_cap_is_bounded_before_the_device():
