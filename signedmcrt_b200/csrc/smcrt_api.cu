@@ -506,6 +506,13 @@ int enqueue(smcrt_ctx* c, long long first, long long count, uint64_t seed, doubl
 // Waits for ev1.  The kernel enforces the context's time limit itself (a
 // %globaltimer budget, after which threads stop between flights and raise
 // STATUS_ABORTED); the host waits that long plus a grace period.
+// Sleep between two polls of a running launch, about 1% of the time waited so far
+// (20 us to 500 us): a short launch is not held up by a long sleep, and a long one
+// costs few polls.
+void poll_sleep(double waited_ms) {
+    std::this_thread::sleep_for(std::chrono::microseconds((long)std::min(500.0, std::max(20.0, waited_ms * 10.0))));
+}
+
 int wait_bounded(smcrt_ctx* c) {
     auto t0 = std::chrono::steady_clock::now();
     const double limit = (double)c->timeout_ms + 30000.0;
@@ -515,7 +522,7 @@ int wait_bounded(smcrt_ctx* c) {
         if (e != cudaErrorNotReady) return fail(SMCRT_ERR_CUDA, std::string("kernel: ") + cudaGetErrorString(e));
         double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         if (ms > limit) return fail(SMCRT_ERR_TIMEOUT, "transport kernel did not finish within its time limit");
-        std::this_thread::sleep_for(std::chrono::microseconds(ms < 10 ? 20 : 500));
+        poll_sleep(ms);
     }
 }
 
@@ -1233,7 +1240,7 @@ int batch_wait(smcrt_batch* b) {
         if (e != cudaErrorNotReady) return fail(SMCRT_ERR_CUDA, std::string("batch kernel: ") + cudaGetErrorString(e));
         double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         if (ms > limit) return fail(SMCRT_ERR_TIMEOUT, "batch kernel did not finish within its time limit");
-        std::this_thread::sleep_for(std::chrono::microseconds(ms < 10 ? 20 : 500));
+        poll_sleep(ms);
     }
 }
 
@@ -1699,7 +1706,7 @@ int run_static_t(const smcrt_scene* scene, const smcrt_grid* grid, const smcrt_s
             if (q != cudaErrorNotReady) return fail(SMCRT_ERR_CUDA, std::string("kernel: ") + cudaGetErrorString(q));
             const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
             if (ms > limit) return fail(SMCRT_ERR_TIMEOUT, "transport kernel did not finish within its time limit");
-            std::this_thread::sleep_for(std::chrono::microseconds(ms < 10 ? 20 : 500));
+            poll_sleep(ms);
         }
     }
     unsigned long long cnt[1 + C_NUM];
