@@ -3,12 +3,18 @@
 Each kernel variant (transport precision x kernel kind) is its own translation
 unit, so the variants compile in parallel; the host API and the probes are two
 more.  Objects are cached under signedmcrt_b200/_build and rebuilt when any
-source or header is newer.
+source or header is newer, or differs from the one the library was built from.
+Next to the library, libsmcrt_b200.build.json records the SHA-256 of every source
+and header it was compiled from, the nvcc version and the flags; the loader
+(`_lib.py`) refuses an in-tree library whose sources have changed since.
 """
 from __future__ import annotations
 
+import hashlib
+import json
 import os
 import shutil
+import time
 import subprocess
 import sys
 from concurrent.futures import ThreadPoolExecutor
@@ -36,6 +42,26 @@ def nvcc() -> str:
 
 def _deps() -> list[Path]:
     return sorted(CSRC.glob("*.cu*")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "smcrt.h"]
+
+
+def manifest_path(lib: Path) -> Path:
+    return lib.with_name(lib.stem + ".build.json")
+
+
+def source_hashes() -> dict[str, str]:
+    """SHA-256 of every source and header the library is compiled from, by path
+    relative to the repository root."""
+    return {str(d.relative_to(ROOT)): hashlib.sha256(d.read_bytes()).hexdigest() for d in _deps()}
+
+
+def _manifest_matches(lib: Path) -> bool:
+    m = manifest_path(lib)
+    if not lib.exists() or not m.exists():
+        return False
+    try:
+        return json.loads(m.read_text()).get("sources") == source_hashes()
+    except (OSError, ValueError):
+        return False
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:
@@ -70,7 +96,10 @@ def build(verbose: bool = False, jobs: int | None = None, extra_flags: list[str]
     deps = _deps()
     exe = nvcc()
     flags = NVCC_FLAGS + (extra_flags or [])
-    todo = [(obj, args) for obj, args in _units() if _stale(obj, deps)]
+    # every unit when the sources differ from the recorded ones (mtimes alone can
+    # miss a change, e.g. files copied with their times kept)
+    fresh = _manifest_matches(LIB)
+    todo = [(obj, args) for obj, args in _units() if not fresh or _stale(obj, deps)]
 
     def run(item):
         obj, args = item
@@ -91,6 +120,12 @@ def build(verbose: bool = False, jobs: int | None = None, extra_flags: list[str]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if todo or not manifest_path(LIB).exists():
+        ver = subprocess.run([exe, "--version"], capture_output=True, text=True).stdout.strip().splitlines()
+        manifest_path(LIB).write_text(json.dumps({
+            "library": LIB.name, "sources": source_hashes(), "nvcc": ver[-1] if ver else "",
+            "flags": flags, "units_compiled": [obj.name for obj, _ in todo],
+            "built_utc": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}, indent=1) + "\n")
     return LIB
 
 

@@ -2,6 +2,7 @@
 include/smcrt.h declares, and the ctypes mirror has the header's struct layout."""
 import ctypes as C
 import json
+import os
 import re
 import subprocess
 from pathlib import Path
@@ -117,6 +118,20 @@ def test_render_checks_its_arguments_before_the_device():
         with pytest.raises(_lib.SmcrtError) as e:
             T.render(arr, (4, 4, 4), (1.0, 1.0, 1.0))
         assert e.value.code == abi.ERR_NO_DEVICE
+
+
+def test_library_provenance_is_checked_on_load(monkeypatch):
+    """The in-tree library carries a manifest of the sources it was built from;
+    the loader accepts it only while those sources are unchanged."""
+    from signedmcrt_b200 import _lib, build
+    if "SMCRT_B200_LIB" in os.environ:
+        pytest.skip("another build of the library is selected")
+    _lib._check_provenance()  # the library built for this test run
+    real = build.source_hashes()
+    some = sorted(real)[0]
+    monkeypatch.setattr(build, "source_hashes", lambda: dict(real, **{some: "0" * 64}))
+    with pytest.raises(RuntimeError, match="built from other sources"):
+        _lib._check_provenance()
 
 
 def test_group_order_is_checked_before_the_device():
