@@ -295,7 +295,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define SMCRT_MIN_BLOCKS 1
 #endif
 #ifndef SMCRT_WALK_SEGMENTS
-#define SMCRT_WALK_SEGMENTS 3
+#define SMCRT_WALK_SEGMENTS 4
 #endif
 // The nearest-region cache (1: built in; 0: every sweep evaluates every region)
 #ifndef SMCRT_NEAREST_CACHE
